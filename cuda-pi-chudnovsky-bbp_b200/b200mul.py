@@ -1,0 +1,151 @@
+"""Python host mirror of the B200 multiply backend (ctypes over libb2m.so).
+
+Mirrors the reference's multiply-backend interface for the ``ntt-cuda`` path
+(include/bignum.h:180-205): ``mul_ntt_cuda(a, b)`` takes and returns
+little-endian u32 limb arrays (numpy), ``cuda_available()`` reports whether the
+backend initialised. Unlike the reference (src/ntt_cuda.cu:182,239-241) there
+is no CPU fallback: every failure raises :class:`B2MError` carrying the C
+status code.
+
+The library is loaded from this directory; importing this module on a machine
+where ``libb2m.so`` has not been built raises immediately.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libb2m.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "b2m.h")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"libb2m.so not built ({LIB_PATH}); run `make -C {HERE}`")
+
+lib = ctypes.CDLL(LIB_PATH)
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_u64 = ctypes.c_uint64
+
+STATUS = {
+    0: "B2M_OK", 1: "B2M_ERR_INVALID_ARGUMENT", 2: "B2M_ERR_NO_DEVICE", 3: "B2M_ERR_NOT_INITIALIZED",
+    4: "B2M_ERR_CUDA", 5: "B2M_ERR_OUT_OF_MEMORY", 6: "B2M_ERR_TOO_LARGE", 7: "B2M_ERR_OUTPUT_TOO_SMALL",
+    8: "B2M_ERR_DEVICE_TIMEOUT", 9: "B2M_ERR_QUEUE_FULL", 10: "B2M_ERR_NOT_FOUND", 11: "B2M_ERR_SHUTDOWN",
+}
+OK, INVALID_ARGUMENT, NO_DEVICE, NOT_INITIALIZED = 0, 1, 2, 3
+CUDA, OUT_OF_MEMORY, TOO_LARGE, OUTPUT_TOO_SMALL, DEVICE_TIMEOUT = 4, 5, 6, 7, 8
+
+
+class B2MError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        self.status = status
+        detail = lib.b2m_last_error().decode()
+        super().__init__(f"{where}: {STATUS.get(status, status)} ({lib.b2m_strerror(status).decode()})"
+                         + (f": {detail}" if detail else ""))
+
+
+def _sig(name, res, args):
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = args
+    return f
+
+
+_sig("b2m_init", ctypes.c_int, [ctypes.c_int, _u64])
+_sig("b2m_shutdown", ctypes.c_int, [])
+_sig("b2m_cuda_available", ctypes.c_int, [])
+_sig("b2m_strerror", ctypes.c_char_p, [ctypes.c_int])
+_sig("b2m_last_error", ctypes.c_char_p, [])
+_sig("b2m_ntt_length", _u64, [_u64, _u64])
+_sig("b2m_workspace_bytes", _u64, [_u64, _u64])
+_sig("b2m_mul_host", ctypes.c_int, [_u32p, _u64, _u32p, _u64, _u32p, _u64, _u64p])
+_sig("b2m_mul_device", ctypes.c_int,
+     [ctypes.c_void_p, _u64, ctypes.c_void_p, _u64, ctypes.c_void_p, _u64, ctypes.c_void_p, ctypes.c_void_p])
+_sig("b2m_stream_check", ctypes.c_int, [ctypes.c_void_p])
+
+
+def check(status: int, where: str) -> None:
+    if status != OK:
+        raise B2MError(status, where)
+
+
+def header_symbols(path: str = HEADER) -> list[str]:
+    """Every function name declared in include/b2m.h (for export checks)."""
+    text = open(path).read()
+    return sorted(set(re.findall(r"\b(b2m_[a-z0-9_]+)\s*\(", text)))
+
+
+def init(device: int = 0, hbm_budget_bytes: int = 0) -> None:
+    check(lib.b2m_init(device, hbm_budget_bytes), "b2m_init")
+
+
+def shutdown() -> None:
+    check(lib.b2m_shutdown(), "b2m_shutdown")
+
+
+def cuda_available() -> bool:
+    """Reference: pidigits::cuda_available() (src/ntt_cuda.cu:165-173)."""
+    return bool(lib.b2m_cuda_available())
+
+
+def ntt_length(na: int, nb: int) -> int:
+    """Reference: ntt_length (include/ntt.h:47-50)."""
+    return int(lib.b2m_ntt_length(na, nb))
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint32))
+
+
+def mul_ntt_cuda(a, b, out: np.ndarray | None = None) -> np.ndarray:
+    """Reference: pidigits::mul_ntt_cuda (src/ntt_cuda.cu:179-243).
+
+    Host arrays in, trimmed product out, synchronous. ``out`` (u32, at least
+    len(a) + len(b) limbs, ideally page-locked) may be supplied to avoid an
+    allocation; the returned array is then a view of it.
+    """
+    a, b = _u32(a), _u32(b)
+    if a.size == 0 or b.size == 0:
+        return np.zeros(0, np.uint32)
+    if out is None:
+        out = np.empty(a.size + b.size, np.uint32)
+    n = _u64(0)
+    check(lib.b2m_mul_host(a.ctypes.data_as(_u32p), a.size, b.ctypes.data_as(_u32p), b.size,
+                           out.ctypes.data_as(_u32p), out.size, ctypes.byref(n)), "b2m_mul_host")
+    return out[: n.value]
+
+
+def mul_device(a_ptr: int, na: int, b_ptr: int, nb: int, out_ptr: int, out_cap: int,
+               out_len_ptr: int = 0, stream: int = 0) -> None:
+    """Device-pointer product ordered on `stream` (raw CUDA handles as ints)."""
+    check(lib.b2m_mul_device(a_ptr, na, b_ptr, nb, out_ptr, out_cap, out_len_ptr or None, stream or None),
+          "b2m_mul_device")
+
+
+def stream_check(stream: int = 0) -> None:
+    check(lib.b2m_stream_check(stream or None), "b2m_stream_check")
+
+
+# ---- seeded operands -----------------------------------------------------------
+# limb i of (seed, n) = high 32 bits of splitmix64's output function applied to
+# seed + (i + 1) * 0x9E3779B97F4A7C15; the top limb is forced non-zero.
+# kind 0 = uniform random limbs, 1 = all 0xFFFFFFFF (worst-case carries).
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+
+
+def gen_operand(seed: int, n: int, kind: int = 0) -> np.ndarray:
+    if kind == 1:
+        return np.full(n, 0xFFFFFFFF, np.uint32)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + (np.arange(1, n + 1, dtype=np.uint64) * _GOLDEN)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    out = (z >> np.uint64(32)).astype(np.uint32)
+    if n and out[-1] == 0:
+        out[-1] = 1
+    return out

@@ -1,0 +1,53 @@
+// b2m_context.h -- the process-wide library context (one device).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <mutex>
+#include <string>
+
+#include "b2m.h"
+#include "b2m_internal.h"
+
+namespace b2m {
+
+struct Context {
+    int device = -1;
+    int sm_count = 0;
+    uint64_t budget = 0;                 // bytes the library may hold on the device
+    std::atomic<uint64_t> in_use{0};     // bytes currently reserved against the budget
+    u64* d_tables = nullptr;             // dtw | u1 | u2, resident
+    RootTables tw{};
+    u32* d_err = nullptr;                // sticky device error word (bounded waits)
+    cudaStream_t hstream = nullptr;      // stream of the host-buffer entry point
+    std::mutex host_mu;                  // serialises b2m_mul_host (shared buffers)
+    void* host_dev = nullptr;            // device buffers of b2m_mul_host, grown on demand
+    uint64_t host_dev_cap = 0;
+};
+
+extern Context* g_ctx;
+extern std::mutex g_ctx_mu;
+
+Context* ctx();
+void set_error(const std::string& msg);
+b2m_status cuda_status(cudaError_t e, const char* what);
+int ilog2_pow2(uint64_t n);
+uint64_t ntt_length_of(uint64_t na, uint64_t nb);
+bool budget_reserve(Context* c, uint64_t bytes);
+void budget_release(Context* c, uint64_t bytes);
+b2m_status check_sizes(uint64_t na, uint64_t nb, int* logn);
+
+// Reads and clears the device error word (caller has synchronised).
+inline b2m_status take_device_error(Context* c) {
+    u32 h = 0;
+    cudaError_t e = cudaMemcpy(&h, c->d_err, sizeof(u32), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMemcpy(error word)");
+    if (h) {
+        cudaMemset(c->d_err, 0, sizeof(u32));
+        set_error("carry lookback wait exceeded its bound");
+        return B2M_ERR_DEVICE_TIMEOUT;
+    }
+    return B2M_OK;
+}
+
+}  // namespace b2m

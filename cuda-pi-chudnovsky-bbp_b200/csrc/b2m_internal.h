@@ -1,0 +1,86 @@
+// b2m_internal.h -- declarations shared by the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "gl.cuh"
+
+namespace b2m {
+
+constexpr int MAX_LOGN = 30;      // coefficients stay below p for N <= 2^32
+constexpr int SMALL_MAX_LOGN = 13; // one CTA holds both transforms up to here
+constexpr int CARRY_THREADS = 256;
+constexpr int CARRY_G = 16;       // coefficients per thread in the carry kernel
+constexpr int CARRY_CHUNK = CARRY_THREADS * CARRY_G;
+// Dynamic shared memory each kernel may request: the largest tile (2^14
+// elements + padding, ~133 KB) fits, and the opt-in limit (227 KB on sm_100)
+// leaves room for the kernels' static shared memory.
+constexpr int kMaxDynSmem = 200 * 1024;
+
+// Device root tables, built once per device and kept resident:
+//   dtw[2^l + e] = w_{2^l}^e, l in [0, 14]          (2^15 entries)
+//   u1[e] = RHO^e, u2[e] = RHO^(e * 2^16), e < 2^16  (2 x 2^16 entries)
+struct RootTables {
+    const u64* dtw;
+    const u64* u1;
+    const u64* u2;
+};
+
+// Pass plan of one transform length.
+struct Plan {
+    int logn = 0;
+    int npass = 0;   // 0 = single-CTA multiply
+    int logr[3] = {0, 0, 0};
+    int logc[3] = {0, 0, 0};
+};
+
+Plan make_plan(int logn);
+
+// Per-product workspace layout (bytes): two N-element u64 arrays plus the
+// carry scratch (lookback slots, ticket, out_len staging).
+struct LookbackSlot {
+    u64 agg_h, agg_t, incl;
+    u32 flag, pad;
+};
+uint64_t workspace_bytes_for(int logn);
+uint64_t carry_scratch_bytes(int logn);
+
+// Kernel launch sequence for one product on `stream`.
+//   a, b: device limbs; out: na+nb limbs; out_len: device u64 (may be null).
+//   ws: workspace of workspace_bytes_for(logn) bytes; err: device error word.
+cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb, u32* out,
+                           uint64_t* out_len, void* ws, const Plan& plan, const RootTables& tw,
+                           u32* err, cudaStream_t stream);
+
+// One-time per-device kernel attribute setup (dynamic shared memory limits).
+cudaError_t configure_kernels();
+
+// Launch geometry of one pass (see make_plan / pass_geo in ntt_launch.cu).
+struct PassGeo {
+    int logr = 0, logc = 0, logs = 0, logm = 0;
+    unsigned grid = 0, block = 0;
+    size_t smem = 0;
+};
+PassGeo pass_geo(const Plan& p, int k);
+
+// Per-family launchers (ntt_fam_*.cu, ntt_carry.cu); each dispatches on the
+// radix exponent to the matching template instantiation.
+cudaError_t launch_fwd_first(int logr, const PassGeo& g, cudaStream_t s, const u32* limbs, u64 ndig, u64* out,
+                             const RootTables& tw);
+cudaError_t launch_fwd_mid(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw);
+cudaError_t launch_inv_mid(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw);
+cudaError_t launch_fwd_last(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw);
+cudaError_t launch_fused_last(int logr, const PassGeo& g, cudaStream_t s, u64* bbuf, const u64* aspec, u64 ninv,
+                              const RootTables& tw);
+cudaError_t launch_mul_small(int logn, const PassGeo& g, cudaStream_t s, const u32* a, u64 na, const u32* b, u64 nb,
+                             u32* out, u64 nout, unsigned long long* out_len, u64 ninv, const RootTables& tw);
+cudaError_t launch_carry(unsigned nchunks, cudaStream_t s, const u64* coef, u32* out, u64 nout,
+                         LookbackSlot* slots, u32* ticket, unsigned long long* out_len, u32* err);
+cudaError_t configure_first();
+cudaError_t configure_mid();
+cudaError_t configure_last();
+cudaError_t configure_fused();
+cudaError_t configure_small();
+
+}  // namespace b2m

@@ -1,0 +1,118 @@
+// gl.cuh -- Goldilocks field GF(p), p = 2^64 - 2^32 + 1, for host and device.
+//
+// Same field as the reference's include/goldilocks.h:83-189 (constants, add,
+// sub, 128-bit Solinas fold, mul, pow, inverse), written afresh for this
+// backend: every function keeps values canonical in [0, p), and multiplication
+// by a power of two (gl_shl) is a shift plus a fold instead of a full multiply,
+// which is what makes the radix-64 register butterflies cheap:
+//   2^64 == 2^32 - 1 (mod p), 2^96 == -1, 2^192 == 1,
+// so 2 has order 192 and 8 = 2^3 is a primitive 64th root of unity.
+//
+// The transform root used throughout is RHO, a primitive 2^32-th root chosen
+// so that RHO^(2^26) == 8. With it every power-of-two root in the transform is
+// a power of RHO and the radix-64 roots are exactly the shift roots, so the
+// register butterflies (shifts) and the table twiddles (powers of RHO) agree.
+// RHO = 7^(5 (p-1) / 2^32); the reference uses 7^((p-1)/N) per size
+// (goldilocks.h:187-189). Only the product integer is defined by the
+// reference, not the spectrum, so the choice of root is free.
+#pragma once
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define GL_FN __host__ __device__ __forceinline__
+#else
+#define GL_FN inline
+#endif
+
+namespace b2m {
+
+typedef unsigned long long u64;
+typedef unsigned int u32;
+
+constexpr u64 GL_P = 0xFFFFFFFF00000001ull;
+constexpr u64 GL_EPS = 0xFFFFFFFFull;  // 2^64 mod p
+constexpr u64 GL_RHO = 0xe2af70635744fd26ull;
+
+GL_FN u64 gl_mulhi(u64 a, u64 b) {
+#if defined(__CUDA_ARCH__)
+    return __umul64hi(a, b);
+#else
+    return (u64)(((unsigned __int128)a * b) >> 64);
+#endif
+}
+
+// a + b for canonical a, b. A carry out of 2^64 is worth EPS; the sum is then
+// below 2p, so one conditional subtract of p canonicalises it.
+GL_FN u64 gl_add(u64 a, u64 b) {
+    u64 s = a + b;
+    u64 t = s + GL_EPS;            // s - p (mod 2^64)
+    bool wrap = s < a;             // a + b >= 2^64
+    return (wrap || s >= GL_P) ? t : s;
+}
+
+// a - b for canonical a, b: a borrow wraps by 2^64 == EPS too many.
+GL_FN u64 gl_sub(u64 a, u64 b) {
+    u64 d = a - b;
+    return (a < b) ? d - GL_EPS : d;
+}
+
+GL_FN u64 gl_neg(u64 a) { return a ? GL_P - a : 0; }
+
+// lo + h * 2^64 for h < 2^32:  == lo + h * EPS, with h*EPS < 2^64.
+GL_FN u64 gl_fold32(u64 lo, u64 h) {
+    u64 t1 = h * GL_EPS;
+    u64 t2 = lo + t1;
+    if (t2 < t1) t2 += GL_EPS;     // the second fold cannot carry again
+    return t2 >= GL_P ? t2 - GL_P : t2;
+}
+
+// Full 128-bit value hi:lo reduced: hi = hh*2^32 + hl contributes
+// hl*2^64 == hl*EPS and hh*2^96 == -hh.
+GL_FN u64 gl_reduce128(u64 lo, u64 hi) {
+    u64 hh = hi >> 32, hl = hi & 0xFFFFFFFFull;
+    u64 t0 = lo - hh;
+    if (lo < hh) t0 -= GL_EPS;
+    return gl_fold32(t0, hl);
+}
+
+GL_FN u64 gl_mul(u64 a, u64 b) { return gl_reduce128(a * b, gl_mulhi(a, b)); }
+
+// x * 2^s for canonical x and 0 <= s < 192. Written so that, with s known at
+// compile time (all register butterflies), every branch folds away.
+GL_FN u64 gl_shl(u64 x, int s) {
+    bool neg = false;
+    if (s >= 96) { s -= 96; neg = true; }   // 2^96 == -1
+    u64 r;
+    if (s == 0) {
+        r = x;
+    } else if (s <= 32) {
+        r = gl_fold32(x << s, x >> (64 - s));
+    } else if (s < 64) {
+        r = gl_reduce128(x << s, x >> (64 - s));
+    } else if (s == 64) {
+        r = gl_reduce128(0, x);
+    } else {
+        // x*2^(s-64) = zl + zh*2^64 (zh < 2^32); times 2^64:
+        // zl*2^64 + zh*2^128 == zl*2^64 - zh*2^32.
+        u64 zl = x << (s - 64), zh = x >> (128 - s);
+        r = gl_sub(gl_reduce128(0, zl), zh << 32);
+    }
+    return neg ? gl_neg(r) : r;
+}
+
+GL_FN u64 gl_pow(u64 b, u64 e) {
+    u64 r = 1;
+    while (e) {
+        if (e & 1) r = gl_mul(r, b);
+        b = gl_mul(b, b);
+        e >>= 1;
+    }
+    return r;
+}
+
+GL_FN u64 gl_inv(u64 a) { return gl_pow(a, GL_P - 2); }
+
+// Primitive 2^l-th root of unity in the RHO chain (l <= 32).
+GL_FN u64 gl_root2(int l) { return gl_pow(GL_RHO, 1ull << (32 - l)); }
+
+}  // namespace b2m

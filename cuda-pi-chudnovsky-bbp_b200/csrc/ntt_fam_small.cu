@@ -1,0 +1,44 @@
+// ntt_fam_small.cu -- instantiations and launchers: single-CTA products, N <= 2^13.
+// Kernel bodies are in ntt_kernels.cuh; one file per family keeps the
+// heavily unrolled instantiations compiling in parallel.
+#include "ntt_kernels.cuh"
+
+namespace b2m {
+
+cudaError_t launch_mul_small(int logn, const PassGeo& g, cudaStream_t s, const u32* a, u64 na, const u32* b, u64 nb, u32* out, u64 nout, unsigned long long* out_len, u64 ninv, const RootTables& tw) {
+    switch (logn) {
+        case 2: k_mul_small<2><<<g.grid, g.block, g.smem, s>>>(a, na, b, nb, out, nout, out_len, ninv, tw); break;
+        case 3: k_mul_small<3><<<g.grid, g.block, g.smem, s>>>(a, na, b, nb, out, nout, out_len, ninv, tw); break;
+        case 4: k_mul_small<4><<<g.grid, g.block, g.smem, s>>>(a, na, b, nb, out, nout, out_len, ninv, tw); break;
+        case 5: k_mul_small<5><<<g.grid, g.block, g.smem, s>>>(a, na, b, nb, out, nout, out_len, ninv, tw); break;
+        case 6: k_mul_small<6><<<g.grid, g.block, g.smem, s>>>(a, na, b, nb, out, nout, out_len, ninv, tw); break;
+        case 7: k_mul_small<7><<<g.grid, g.block, g.smem, s>>>(a, na, b, nb, out, nout, out_len, ninv, tw); break;
+        case 8: k_mul_small<8><<<g.grid, g.block, g.smem, s>>>(a, na, b, nb, out, nout, out_len, ninv, tw); break;
+        case 9: k_mul_small<9><<<g.grid, g.block, g.smem, s>>>(a, na, b, nb, out, nout, out_len, ninv, tw); break;
+        case 10: k_mul_small<10><<<g.grid, g.block, g.smem, s>>>(a, na, b, nb, out, nout, out_len, ninv, tw); break;
+        case 11: k_mul_small<11><<<g.grid, g.block, g.smem, s>>>(a, na, b, nb, out, nout, out_len, ninv, tw); break;
+        case 12: k_mul_small<12><<<g.grid, g.block, g.smem, s>>>(a, na, b, nb, out, nout, out_len, ninv, tw); break;
+        case 13: k_mul_small<13><<<g.grid, g.block, g.smem, s>>>(a, na, b, nb, out, nout, out_len, ninv, tw); break;
+        default: return cudaErrorInvalidConfiguration;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t configure_small() {
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mul_small<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mul_small<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mul_small<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mul_small<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mul_small<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mul_small<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mul_small<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mul_small<9>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mul_small<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mul_small<11>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mul_small<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mul_small<13>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    return e;
+}
+
+}  // namespace b2m

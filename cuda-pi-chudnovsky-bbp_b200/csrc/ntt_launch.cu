@@ -1,0 +1,137 @@
+// ntt_launch.cu -- pass plans and the launch sequence of one product.
+//
+// For N = 2^L >= 2^14 (a 2- or 3-pass plan):
+//   A: first pass (u32 limbs -> 16-bit digits), middle passes, last pass
+//      (spectrum register-major per CTA);
+//   B: first pass, middle passes, fused last pass (B's last forward pass,
+//      pointwise product with A's spectrum and N^-1, first inverse pass);
+//   inverse middle/first passes (pass 1 yields the coefficients), then the
+//   decoupled-lookback carry into u32 limbs and the trimmed length.
+// For N <= 2^13 a single CTA does everything.
+//
+// Reference counterpart: mul_ntt_cuda (src/ntt_cuda.cu:179-243) -- host
+// repack (include/ntt.h:56-64), bit reversal + log2 N radix-2 launches per
+// transform, pointwise (:117-121), scale (:124-128), host carry
+// (include/ntt.h:70-91) -- all replaced by the sequence below.
+#include <cuda_runtime.h>
+
+#include "b2m_internal.h"
+#include "carry.cuh"
+
+namespace b2m {
+
+Plan make_plan(int logn) {
+    Plan p;
+    p.logn = logn;
+    if (logn <= SMALL_MAX_LOGN) {
+        p.npass = 0;
+        return p;
+    }
+    if (logn <= 26) {
+        // Two passes; the first keeps at least 4 columns (32-byte rows) in a
+        // 2^14-element tile, the last (contiguous) pass takes up to 2^14.
+        p.npass = 2;
+        p.logr[0] = logn / 2 < 12 ? logn / 2 : 12;
+        p.logr[1] = logn - p.logr[0];
+    } else {
+        p.npass = 3;
+        p.logr[0] = logn / 3;
+        p.logr[1] = logn / 3;
+        p.logr[2] = logn - 2 * (logn / 3);
+    }
+    const int tile = logn >= 20 ? 14 : (logn >= 17 ? 13 : 12);
+    int before = 0;
+    for (int k = 0; k < p.npass; ++k) {
+        const int r = p.logr[k];
+        const int after = logn - before - r;  // log2 S
+        int c = tile - r;
+        if (c < 0) c = 0;
+        const int cap = (k + 1 < p.npass) ? after : (logn - r);
+        if (c > cap) c = cap;
+        p.logc[k] = c;
+        before += r;
+    }
+    return p;
+}
+
+PassGeo pass_geo(const Plan& p, int k) {
+    int before = 0;
+    for (int i = 0; i < k; ++i) before += p.logr[i];
+    PassGeo g;
+    g.logr = p.logr[k];
+    g.logc = p.logc[k];
+    g.logs = p.logn - before - g.logr;
+    g.logm = g.logr + g.logs;
+    g.grid = (unsigned)(1ull << (p.logn - g.logr - g.logc));
+    g.block = (unsigned)(1u << (g.logr + g.logc - 6));
+    const size_t rp = (size_t)(1 << g.logr) + (size_t)((1 << g.logr) >> 6);
+    g.smem = rp * ((size_t)1 << g.logc) * sizeof(u64);
+    return g;
+}
+
+uint64_t carry_scratch_bytes(int logn) {
+    const uint64_t chunks = logn >= 12 ? (1ull << logn) / CARRY_CHUNK : 1;
+    return chunks * sizeof(LookbackSlot) + 256;
+}
+
+uint64_t workspace_bytes_for(int logn) {
+    if (logn <= SMALL_MAX_LOGN) return 256;
+    return 2 * (8ull << logn) + carry_scratch_bytes(logn);
+}
+
+cudaError_t configure_kernels() {
+    cudaError_t e = configure_first();
+    if (e == cudaSuccess) e = configure_mid();
+    if (e == cudaSuccess) e = configure_last();
+    if (e == cudaSuccess) e = configure_fused();
+    if (e == cudaSuccess) e = configure_small();
+    return e;
+}
+
+static cudaError_t launch_forward(const u32* limbs, uint64_t nlimbs, u64* buf, const Plan& p,
+                                  const RootTables& tw, bool fused, const u64* aspec, u64 ninv,
+                                  cudaStream_t s) {
+    cudaError_t e = launch_fwd_first(p.logr[0], pass_geo(p, 0), s, limbs, 2 * nlimbs, buf, tw);
+    for (int k = 1; e == cudaSuccess && k + 1 < p.npass; ++k) e = launch_fwd_mid(p.logr[k], pass_geo(p, k), s, buf, tw);
+    if (e != cudaSuccess) return e;
+    const int last = p.npass - 1;
+    return fused ? launch_fused_last(p.logr[last], pass_geo(p, last), s, buf, aspec, ninv, tw)
+                 : launch_fwd_last(p.logr[last], pass_geo(p, last), s, buf, tw);
+}
+
+cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb, u32* out, uint64_t* out_len,
+                           void* ws, const Plan& p, const RootTables& tw, u32* err, cudaStream_t s) {
+    const int logn = p.logn;
+    const u64 ninv = gl_inv(1ull << logn);
+    const u64 nout = na + nb;
+    if (p.npass == 0) {
+        PassGeo g{};
+        const int T = logn >= 6 ? (1 << (logn - 6)) : 1;
+        const size_t rp = (size_t)(1 << logn) + (size_t)((1 << logn) >> 6);
+        g.grid = 1;
+        g.block = (unsigned)T;
+        g.smem = 2 * rp * sizeof(u64) + (size_t)T * 2 * sizeof(u64);
+        return launch_mul_small(logn, g, s, a, na, b, nb, out, nout,
+                                reinterpret_cast<unsigned long long*>(out_len), ninv, tw);
+    }
+    const uint64_t n = 1ull << logn;
+    u64* bufA = static_cast<u64*>(ws);
+    u64* bufB = bufA + n;
+    unsigned char* scratch = reinterpret_cast<unsigned char*>(bufB + n);
+    const uint64_t nchunks = n / CARRY_CHUNK;
+    LookbackSlot* slots = reinterpret_cast<LookbackSlot*>(scratch);
+    u32* ticket = reinterpret_cast<u32*>(scratch + nchunks * sizeof(LookbackSlot));
+    unsigned long long* len_tmp = reinterpret_cast<unsigned long long*>(ticket + 2);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, carry_scratch_bytes(logn), s);
+    if (e != cudaSuccess) return e;
+    unsigned long long* ol = out_len ? reinterpret_cast<unsigned long long*>(out_len) : len_tmp;
+    if (out_len && (e = cudaMemsetAsync(out_len, 0, sizeof(uint64_t), s)) != cudaSuccess) return e;
+
+    if ((e = launch_forward(a, na, bufA, p, tw, false, nullptr, 0, s)) != cudaSuccess) return e;
+    if ((e = launch_forward(b, nb, bufB, p, tw, true, bufA, ninv, s)) != cudaSuccess) return e;
+    for (int k = p.npass - 2; k >= 0; --k)
+        if ((e = launch_inv_mid(p.logr[k], pass_geo(p, k), s, bufB, tw)) != cudaSuccess) return e;
+    return launch_carry((unsigned)nchunks, s, bufB, out, nout, slots, ticket, ol, err);
+}
+
+}  // namespace b2m

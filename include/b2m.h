@@ -1,0 +1,110 @@
+/*
+ * b2m.h -- C ABI of the B200 Goldilocks-NTT big-integer multiply backend.
+ *
+ * Numbers are little-endian arrays of 32-bit limbs (value = sum limb[i] *
+ * 2^(32 i)), exactly the magnitude layout of the reference's BigInt::mag
+ * (include/bignum.h:21-44, 106-109). Products are bit-exact: the same integer
+ * the reference's mul_ntt_cpu / mul_schoolbook return, trimmed of leading
+ * zero limbs. No entry point ever falls back to a CPU multiply; failures are
+ * reported as status codes.
+ *
+ * The reference exposes this path as C++ functions
+ *   std::vector<uint32_t> pidigits::mul_ntt_cuda(const std::vector<uint32_t>&,
+ *                                                const std::vector<uint32_t>&)
+ *   bool pidigits::cuda_available()
+ * (include/bignum.h:200-205, src/ntt_cuda.cu:165-243). The C++ shim
+ * ntt_cuda_b200.cpp maps those two signatures onto b2m_mul_host and
+ * b2m_cuda_available below, so the reference's own callers (mul_dispatch in
+ * src/bignum.cpp:204-232, chudnovsky_bs in src/chudnovsky.cpp:64-102) run on
+ * this backend unchanged.
+ *
+ * Threading: every entry point may be called from any host thread; library
+ * state is guarded internally. Device work of the *_device / batch calls is
+ * ordered on the caller's stream.
+ */
+#ifndef B2M_H
+#define B2M_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B2M_API_VERSION 1
+
+/* A CUDA stream (cudaStream_t / CUstream); NULL is the legacy default stream. */
+typedef struct CUstream_st* b2m_stream;
+
+typedef enum b2m_status {
+    B2M_OK = 0,
+    B2M_ERR_INVALID_ARGUMENT = 1,  /* null pointer with a non-zero size, bad flag, ... */
+    B2M_ERR_NO_DEVICE = 2,         /* no CUDA device, or not an sm_100 device */
+    B2M_ERR_NOT_INITIALIZED = 3,   /* b2m_init was not called (or failed) */
+    B2M_ERR_CUDA = 4,              /* a CUDA runtime call failed (detail: b2m_last_error) */
+    B2M_ERR_OUT_OF_MEMORY = 5,     /* device allocation failed or the HBM budget is exhausted */
+    B2M_ERR_TOO_LARGE = 6,         /* transform length above 2^30 (na + nb > 2^28 limbs) */
+    B2M_ERR_OUTPUT_TOO_SMALL = 7,  /* out_cap < na + nb */
+    B2M_ERR_DEVICE_TIMEOUT = 8,    /* a bounded device-side wait gave up (carry lookback) */
+    B2M_ERR_QUEUE_FULL = 9,        /* serving: request table full */
+    B2M_ERR_NOT_FOUND = 10,        /* serving: unknown ticket */
+    B2M_ERR_SHUTDOWN = 11          /* serving: the server is stopping */
+} b2m_status;
+
+/* ---- lifetime ------------------------------------------------------------ */
+
+/* Replaces the implicit per-call setup of src/ntt_cuda.cu:179-214 (device
+ * probe, cudaMalloc, twiddle build). Selects `device`, uploads the resident
+ * root tables once and sets the HBM budget the library may allocate
+ * (0 = 90% of the device's free memory at init). Idempotent for the same
+ * device; a second call with another device re-initialises. */
+b2m_status b2m_init(int device, uint64_t hbm_budget_bytes);
+
+/* Frees every device resource the library holds. */
+b2m_status b2m_shutdown(void);
+
+/* Replaces pidigits::cuda_available() (src/ntt_cuda.cu:165-173): 1 when
+ * b2m_init(0, 0) succeeds (or an earlier init succeeded), else 0. Cached. */
+int b2m_cuda_available(void);
+
+/* Human-readable name of a status; never NULL. */
+const char* b2m_strerror(b2m_status status);
+
+/* Detail of the last failure on the calling thread ("" if none). */
+const char* b2m_last_error(void);
+
+/* Replaces ntt_length (include/ntt.h:47-50): next power of two >= 2na + 2nb. */
+uint64_t b2m_ntt_length(uint64_t na, uint64_t nb);
+
+/* Device workspace in bytes that one product of na x nb limbs needs. */
+uint64_t b2m_workspace_bytes(uint64_t na, uint64_t nb);
+
+/* ---- single products ------------------------------------------------------- */
+
+/* Replaces pidigits::mul_ntt_cuda (src/ntt_cuda.cu:179-243): host buffers in,
+ * host buffer out, synchronous. a/b may carry leading zero limbs (their sizes
+ * are taken as given, like the reference's .size()). out must hold
+ * out_cap >= na + nb limbs; *out_len receives the trimmed length (0 for a
+ * zero product or an empty input). Only out[0, *out_len) is defined. */
+b2m_status b2m_mul_host(const uint32_t* a, uint64_t na, const uint32_t* b, uint64_t nb,
+                        uint32_t* out, uint64_t out_cap, uint64_t* out_len);
+
+/* The same product with operands already resident in device memory, ordered
+ * on `stream` and asynchronous: d_out receives na + nb limbs (the limbs past
+ * the trimmed length are zero) and *d_out_len (a device pointer, may be NULL)
+ * the trimmed length. The workspace is taken from a stream-ordered pool.
+ * Device-side failures surface through b2m_stream_check. */
+b2m_status b2m_mul_device(const uint32_t* d_a, uint64_t na, const uint32_t* d_b, uint64_t nb,
+                          uint32_t* d_out, uint64_t out_cap, uint64_t* d_out_len,
+                          b2m_stream stream);
+
+/* Synchronises `stream` and reports (and clears) any device-side failure
+ * raised by this library's kernels since the last check. */
+b2m_status b2m_stream_check(b2m_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B2M_H */
