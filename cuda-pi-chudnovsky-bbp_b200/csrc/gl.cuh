@@ -41,19 +41,44 @@ GL_FN u64 gl_mulhi(u64 a, u64 b) {
 #endif
 }
 
-// a + b for canonical a, b. A carry out of 2^64 is worth EPS; the sum is then
-// below 2p, so one conditional subtract of p canonicalises it.
+// a - b for a < 2^64, b <= p: a borrow wraps by 2^64 == EPS too many, and
+// since b - a <= p the corrected value cannot borrow again. Canonical when
+// a is. The device version is one 32-bit borrow chain: the borrow itself,
+// materialised as 0 or 0xFFFFFFFF (= EPS), is what gets subtracted.
+GL_FN u64 gl_sub(u64 a, u64 b) {
+#if defined(__CUDA_ARCH__)
+    u32 d0, d1, m;
+    asm("sub.cc.u32 %0, %3, %5;\n\t"
+        "subc.cc.u32 %1, %4, %6;\n\t"
+        "subc.u32 %2, 0, 0;\n\t"
+        "sub.cc.u32 %0, %0, %2;\n\t"
+        "subc.u32 %1, %1, 0;\n\t"
+        : "=r"(d0), "=r"(d1), "=r"(m)
+        : "r"((u32)a), "r"((u32)(a >> 32)), "r"((u32)b), "r"((u32)(b >> 32)));
+    return ((u64)d1 << 32) | d0;
+#else
+    u64 d = a - b;
+    return (a < b) ? d - GL_EPS : d;
+#endif
+}
+
+// a + b for canonical a, b, computed as a - (p - b) (p - b <= p, so gl_sub
+// applies): two instructions for p - b and the borrow chain of gl_sub,
+// instead of an add followed by two range checks.
 GL_FN u64 gl_add(u64 a, u64 b) {
+#if defined(__CUDA_ARCH__)
+    u32 n0, n1;
+    asm("sub.cc.u32 %0, 1, %2;\n\t"
+        "subc.u32 %1, -1, %3;\n\t"
+        : "=r"(n0), "=r"(n1)
+        : "r"((u32)b), "r"((u32)(b >> 32)));
+    return gl_sub(a, ((u64)n1 << 32) | n0);
+#else
     u64 s = a + b;
     u64 t = s + GL_EPS;            // s - p (mod 2^64)
     bool wrap = s < a;             // a + b >= 2^64
     return (wrap || s >= GL_P) ? t : s;
-}
-
-// a - b for canonical a, b: a borrow wraps by 2^64 == EPS too many.
-GL_FN u64 gl_sub(u64 a, u64 b) {
-    u64 d = a - b;
-    return (a < b) ? d - GL_EPS : d;
+#endif
 }
 
 GL_FN u64 gl_neg(u64 a) { return a ? GL_P - a : 0; }

@@ -63,7 +63,9 @@ PassGeo pass_geo(const Plan& p, int k) {
     g.logs = p.logn - before - g.logr;
     g.logm = g.logr + g.logs;
     g.grid = (unsigned)(1ull << (p.logn - g.logr - g.logc));
-    g.block = (unsigned)(1u << (g.logr + g.logc - 6));
+    // 16 elements per thread (two 8-point tasks per radix-8 level), <= 1024.
+    const int logt = g.logr + g.logc - 4;
+    g.block = (unsigned)(1u << (logt < 10 ? logt : 10));
     const size_t rp = (size_t)(1 << g.logr) + (size_t)((1 << g.logr) >> 6);
     g.smem = rp * ((size_t)1 << g.logc) * sizeof(u64);
     return g;
@@ -106,7 +108,7 @@ cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb,
     const u64 nout = na + nb;
     if (p.npass == 0) {
         PassGeo g{};
-        const int T = logn >= 6 ? (1 << (logn - 6)) : 1;
+        const int T = logn >= 4 ? (1 << (logn - 4)) : 1;
         const size_t rp = (size_t)(1 << logn) + (size_t)((1 << logn) >> 6);
         g.grid = 1;
         g.block = (unsigned)T;
