@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Goldilocks-NTT big-integer multiply.
+
+Headline metric: ms per 2^24 x 2^24-limb multiply (seeded uniform random u32
+limbs), device-resident operands, bit-exact product. One "step" is one full
+product (repack, 3 transforms, pointwise, carry, trimmed length) per GPU.
+
+    python bench.py [--gpus N --steps K --warmup W]
+    python -m torch.distributed.run --nnodes=1 --nproc-per-node N --master-addr 127.0.0.1 \\
+        --master-port P bench.py --gpus N --steps K --warmup W
+    python bench.py --impl reference ...   # the reference's own CPU NTT, all host threads
+
+Products are independent, so N GPUs run N products per step with no
+collective on the data path (weak scaling); the step time is the maximum over
+ranks of CUDA-event times, and `value` is that time divided by the products
+all ranks completed. The JSON line also carries the end-to-end figure through
+the host-buffer C-ABI call (pinned host memory, copies in the timed region),
+the roofline of the dominant kernel (CUDA events around each launch), the
+reference's CPU NTT timed on this host, and SM clocks sampled during timing.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "cuda-pi-chudnovsky-bbp_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "ms per 2^24-limb multiply"
+NA = NB = 1 << 24
+SEED_A, SEED_B = 24001, 24002
+
+
+def algorithmic_bytes(na: int, nb: int, n: int) -> int:
+    """Minimum HBM traffic of one product: u32 operands in and product out
+    (8(na+nb)) plus eight N-element u64 sweeps (64N) of a two-pass schedule."""
+    return 8 * (na + nb) + 64 * n
+
+
+def kernel_bytes(kind: str, na: int, nb: int, n: int, operand: int) -> int:
+    """Algorithmic bytes of one launch of each kernel kind (N = transform length)."""
+    if kind == "fwd_first":
+        return 4 * operand + 8 * n
+    if kind in ("fwd_mid", "fwd_last", "inv_mid"):
+        return 16 * n
+    if kind == "fused_last":
+        return 24 * n
+    if kind == "carry":
+        return 8 * n + 4 * (na + nb)
+    return 8 * (na + nb)  # mul_small
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json: copy bandwidth)"
+    return 6650.0, "fallback (6.65 TB/s, earlier pool measurement)"
+
+
+# ---------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+# ---------------------------------------------------------------------------- CPU
+def _ref_or_port():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # the checker: only the CPU-baseline leg of this script uses it
+
+    if oracle.ref_available():
+        return oracle, "reference", lambda a, b: oracle.mul_ref(a, b, "ntt-cpu")
+    return oracle, "port", lambda a, b: oracle.mul_port(a, b)
+
+
+def nlogn_scale(n_from: int, n_to: int) -> float:
+    """Scale a product time from na = nb = n_from to n_to limbs by N log2 N."""
+    nf, nt = 4 * n_from, 4 * n_to  # transform lengths
+    return (nt * math.log2(nt)) / (nf * math.log2(nf))
+
+
+def cpu_products(sample_limbs: int, threads: int, fn) -> float:
+    """Run `threads` concurrent sample products (ctypes releases the GIL);
+    returns the wall time in seconds."""
+    import numpy as np
+    from b200mul import gen_operand
+
+    ops = [(gen_operand(SEED_A + i, sample_limbs), gen_operand(SEED_B + i, sample_limbs)) for i in range(threads)]
+    res = [None] * threads
+
+    def work(i):
+        res[i] = fn(*ops[i])
+
+    ts = [threading.Thread(target=work, args=(i,)) for i in range(threads)]
+    t0 = time.perf_counter()
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    dt = time.perf_counter() - t0
+    assert all(r is not None and r.size == 2 * sample_limbs for r in res) and np is not None
+    return dt
+
+
+def cpu_baseline(sample_log: int = 22) -> dict:
+    """The reference's CPU NTT (single-threaded, as the reference is) on one
+    sample product, scaled to the 2^24-limb metric by N log2 N."""
+    _, kind, fn = _ref_or_port()
+    n = 1 << sample_log
+    dt = cpu_products(n, 1, fn)
+    scale = nlogn_scale(n, NA)
+    return {"value": round(dt * 1e3 * scale, 1), "unit": "ms", "cores": 1, "kind": kind,
+            "sample": f"one {n}x{n}-limb product (mul_ntt_cpu, 1 thread) in {dt:.2f} s, scaled to "
+                      f"2^24 limbs by N log2 N (x{scale:.2f})"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    _, kind, fn = _ref_or_port()
+    threads = os.cpu_count() or 1
+    # Size each step so that warmup + steps stay near two minutes.
+    budget = 120.0 / max(1, args.steps + args.warmup)
+    t_cal = cpu_products(1 << 16, 1, fn)
+    lg = 16
+    while lg < 24 and t_cal * nlogn_scale(1 << 16, 1 << (lg + 1)) * 1.15 <= budget:
+        lg += 1
+    n = 1 << lg
+    for _ in range(args.warmup):
+        cpu_products(n, threads, fn)
+    times = [cpu_products(n, threads, fn) for _ in range(args.steps)]
+    step = statistics.mean(times)
+    scale = nlogn_scale(n, NA)
+    value = step / threads * 1e3 * scale
+    out = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": "ms", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step * 1e3, 2),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (GF(p), p=2^64-2^32+1)",
+        "data": "synthetic: seeded uniform random u32 limbs",
+        "config": {"workload": "2^24 x 2^24-limb product, uniform random limbs", "na": NA, "nb": NB,
+                   "sample_limbs": n, "threads": threads},
+        "cpu_baseline": {"value": round(value, 2), "unit": "ms", "cores": threads, "kind": kind,
+                         "sample": f"each step: {threads} concurrent {n}x{n}-limb products of the reference's "
+                                   f"mul_ntt_cpu (src/ntt_cpu.cpp:111-129), one per host thread; ms per product "
+                                   f"= step wall / {threads}, scaled to 2^24 limbs by N log2 N (x{scale:.2f})"},
+        "e2e": {"value": round(value, 2), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------- ours
+def run_ours(args) -> None:
+    import numpy as np
+    import torch
+
+    import b200mul
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    b200mul.init(local)
+    na, nb = args.na, args.nb
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    a_h = b200mul.gen_operand(SEED_A + 1000 * rank, na)
+    b_h = b200mul.gen_operand(SEED_B + 1000 * rank, nb)
+    a = torch.from_numpy(a_h.view(np.int32)).cuda()
+    b = torch.from_numpy(b_h.view(np.int32)).cuda()
+    out = torch.empty(na + nb, dtype=torch.int32, device="cuda")
+    olen = torch.zeros(1, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    plan = b200mul.plan_describe(na, nb)
+    n = 1 << plan["ntt_log2"]
+
+    def product():
+        b200mul.mul_device(a.data_ptr(), na, b.data_ptr(), nb, out.data_ptr(), na + nb, olen.data_ptr(), sp)
+
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            product()
+    b200mul.stream_check(sp)
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        product()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    b200mul.stream_check(sp)
+    step_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+
+    # Per-kernel device times (CUDA events around each launch on `stream`).
+    traces = [b200mul.mul_device_traced(a.data_ptr(), na, b.data_ptr(), nb, out.data_ptr(), na + nb,
+                                        olen.data_ptr(), sp) for _ in range(args.trace_steps)]
+    per_kind: dict[str, list[float]] = {}
+    per_launch_bytes: dict[str, int] = {}
+    first_seen = 0
+    for tr in traces:
+        first_seen = 0
+        for kind, logr, ms in tr:
+            key = f"{kind}<{logr}>" if kind not in ("carry",) else kind
+            operand = na if (kind == "fwd_first" and first_seen == 0) else nb
+            if kind == "fwd_first":
+                first_seen += 1
+            per_kind.setdefault(key, []).append(ms)
+            per_launch_bytes[key] = kernel_bytes(kind, na, nb, n, operand)
+    kinds = {k: {"launches_per_product": len(v) // len(traces), "avg_ms": statistics.mean(v),
+                 "share": sum(v) / sum(sum(x) for x in per_kind.values())} for k, v in per_kind.items()}
+    dominant = max(kinds, key=lambda k: kinds[k]["avg_ms"] * kinds[k]["launches_per_product"])
+    peak, peak_src = load_peaks()
+    dom_ms = kinds[dominant]["avg_ms"]
+    dom_bytes = per_launch_bytes[dominant]
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    prod_bytes = algorithmic_bytes(na, nb, n)
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(dominant)
+
+    # End to end through the public host-buffer call: pinned host operands,
+    # H2D + product + D2H of the result inside the timed region.
+    pa = torch.empty(na, dtype=torch.int32, pin_memory=True)
+    pb = torch.empty(nb, dtype=torch.int32, pin_memory=True)
+    po = torch.empty(na + nb, dtype=torch.int32, pin_memory=True)
+    pa.numpy()[:] = a_h.view(np.int32)
+    pb.numpy()[:] = b_h.view(np.int32)
+    ha, hb, ho = pa.numpy().view(np.uint32), pb.numpy().view(np.uint32), po.numpy().view(np.uint32)
+    for _ in range(2):
+        res = b200mul.mul_ntt_cuda(ha, hb, out=ho)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        res = b200mul.mul_ntt_cuda(ha, hb, out=ho)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.e2e_steps
+    barrier()
+    e2e_ms = max_over_ranks(e2e_ms)
+    dev = out.cpu().numpy().view(np.uint32)[: int(olen.item())]
+    if not np.array_equal(dev, res):
+        raise RuntimeError("device-resident and host-buffer products differ")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_sample_log)
+
+    if rank == 0:
+        value = step_ms / world
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(step_ms, 4), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64 (GF(p), p=2^64-2^32+1)",
+            "data": "synthetic: seeded uniform random u32 limbs (splitmix64), top limb non-zero",
+            "config": {"workload": "2^24 x 2^24-limb product, uniform random limbs", "na": na, "nb": nb,
+                       "ntt_length": n, "plan": plan, "products_per_step": world,
+                       "glimbs_per_s": round((na + nb) * world / (step_ms * 1e-3) / 1e9, 3),
+                       "l2": f"working set {(4 * (na + nb) * 2 + 16 * n) / 2**20:.0f} MiB per product "
+                             "> 126 MB L2: no flush needed"},
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": round(dom_ms, 4),
+                         "peak_source": peak_src,
+                         "product": {"algorithmic_bytes": prod_bytes,
+                                     "achieved_gbs": round(prod_bytes / (step_ms * 1e-3) / 1e9, 1),
+                                     "frac": round(prod_bytes / (step_ms * 1e-3) / 1e9 / peak, 4)},
+                         "kernels": {k: {"avg_ms": round(v["avg_ms"], 4), "share": round(v["share"], 4),
+                                         "launches_per_product": v["launches_per_product"]}
+                                     for k, v in kinds.items()}},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": 4 * (na + nb) * world,
+                    "d2h_bytes_per_step": (4 * (na + nb) + 8) * world,
+                    "path": "b2m_mul_host (C ABI), pinned host buffers, wall clock per call"},
+            "gpu_launches": plan["launches"] * args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--na", type=int, default=NA)
+    ap.add_argument("--nb", type=int, default=NB)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--trace-steps", type=int, default=10)
+    ap.add_argument("--cpu-sample-log", type=int, default=22)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

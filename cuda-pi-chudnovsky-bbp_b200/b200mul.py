@@ -68,6 +68,24 @@ _sig("b2m_mul_device", ctypes.c_int,
 _sig("b2m_stream_check", ctypes.c_int, [ctypes.c_void_p])
 
 
+class PlanDesc(ctypes.Structure):
+    _fields_ = [("ntt_log2", ctypes.c_uint32), ("npass", ctypes.c_uint32), ("logr", ctypes.c_uint32 * 3),
+                ("logc", ctypes.c_uint32 * 3), ("launches", ctypes.c_uint32)]
+
+
+class KernelTime(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_uint32), ("logr", ctypes.c_uint32), ("ms", ctypes.c_float)]
+
+
+KERNEL_KINDS = {1: "fwd_first", 2: "fwd_mid", 3: "fwd_last", 4: "fused_last", 5: "inv_mid", 6: "carry",
+                7: "mul_small"}
+
+_sig("b2m_plan_describe", ctypes.c_int, [_u64, _u64, ctypes.POINTER(PlanDesc)])
+_sig("b2m_mul_device_traced", ctypes.c_int,
+     [ctypes.c_void_p, _u64, ctypes.c_void_p, _u64, ctypes.c_void_p, _u64, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.POINTER(KernelTime), ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)])
+
+
 def check(status: int, where: str) -> None:
     if status != OK:
         raise B2MError(status, where)
@@ -149,3 +167,20 @@ def gen_operand(seed: int, n: int, kind: int = 0) -> np.ndarray:
     if n and out[-1] == 0:
         out[-1] = 1
     return out
+
+
+def plan_describe(na: int, nb: int) -> dict:
+    d = PlanDesc()
+    check(lib.b2m_plan_describe(na, nb, ctypes.byref(d)), "b2m_plan_describe")
+    return {"ntt_log2": d.ntt_log2, "npass": d.npass, "logr": list(d.logr)[: max(d.npass, 1)],
+            "logc": list(d.logc)[: max(d.npass, 1)], "launches": d.launches}
+
+
+def mul_device_traced(a_ptr: int, na: int, b_ptr: int, nb: int, out_ptr: int, out_cap: int,
+                      out_len_ptr: int = 0, stream: int = 0) -> list[tuple[str, int, float]]:
+    """Device product with per-launch CUDA-event times: [(kind, logr, ms), ...]."""
+    times = (KernelTime * 16)()
+    n = ctypes.c_uint32(0)
+    check(lib.b2m_mul_device_traced(a_ptr, na, b_ptr, nb, out_ptr, out_cap, out_len_ptr or None, stream or None,
+                                    times, 16, ctypes.byref(n)), "b2m_mul_device_traced")
+    return [(KERNEL_KINDS[times[i].kind], times[i].logr, times[i].ms) for i in range(n.value)]

@@ -254,6 +254,68 @@ b2m_status b2m_mul_device(const uint32_t* d_a, uint64_t na, const uint32_t* d_b,
     return cuda_status(e2, "cudaFreeAsync(workspace)");
 }
 
+b2m_status b2m_plan_describe(uint64_t na, uint64_t nb, b2m_plan_desc* d) {
+    if (!d || na == 0 || nb == 0) return B2M_ERR_INVALID_ARGUMENT;
+    int logn;
+    b2m_status st = check_sizes(na, nb, &logn);
+    if (st != B2M_OK) return st;
+    const Plan p = make_plan(logn);
+    d->ntt_log2 = (uint32_t)logn;
+    d->npass = (uint32_t)p.npass;
+    for (int k = 0; k < 3; ++k) {
+        d->logr[k] = (uint32_t)p.logr[k];
+        d->logc[k] = (uint32_t)p.logc[k];
+    }
+    d->launches = (uint32_t)plan_launches(p);
+    return B2M_OK;
+}
+
+b2m_status b2m_mul_device_traced(const uint32_t* d_a, uint64_t na, const uint32_t* d_b, uint64_t nb,
+                                 uint32_t* d_out, uint64_t out_cap, uint64_t* d_out_len, b2m_stream stream,
+                                 b2m_kernel_time* times, uint32_t cap, uint32_t* n) {
+    Context* c = ctx();
+    if (!c) return B2M_ERR_NOT_INITIALIZED;
+    if (!d_a || !d_b || !d_out || !times || !n || na == 0 || nb == 0) return B2M_ERR_INVALID_ARGUMENT;
+    if (out_cap < na + nb) return B2M_ERR_OUTPUT_TOO_SMALL;
+    int logn;
+    b2m_status st = check_sizes(na, nb, &logn);
+    if (st != B2M_OK) return st;
+    cudaSetDevice(c->device);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const Plan p = make_plan(logn);
+    const uint64_t wsb = workspace_bytes_for(logn);
+    if (!budget_reserve(c, wsb)) {
+        set_error("HBM budget exhausted");
+        return B2M_ERR_OUT_OF_MEMORY;
+    }
+    void* ws = nullptr;
+    cudaError_t e = cudaMallocAsync(&ws, wsb, s);
+    if (e != cudaSuccess) {
+        budget_release(c, wsb);
+        return cuda_status(e, "cudaMallocAsync(workspace)");
+    }
+    Tracer tr;
+    for (int i = 0; i <= Tracer::CAP; ++i) cudaEventCreate(&tr.ev[i]);
+    e = launch_product(d_a, na, d_b, nb, d_out, d_out_len, ws, p, c->tw, c->d_err, s, &tr);
+    cudaFreeAsync(ws, s);
+    budget_release(c, wsb);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) {
+        uint32_t k = 0;
+        for (int i = 0; i < tr.n && k < cap; ++i, ++k) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, tr.ev[i], tr.ev[i + 1]);
+            times[k].kind = tr.kind[i];
+            times[k].logr = tr.logr[i];
+            times[k].ms = ms;
+        }
+        *n = k;
+    }
+    for (int i = 0; i <= Tracer::CAP; ++i) cudaEventDestroy(tr.ev[i]);
+    if (e != cudaSuccess) return cuda_status(e, "traced product");
+    return take_device_error(c);
+}
+
 b2m_status b2m_stream_check(b2m_stream stream) {
     Context* c = ctx();
     if (!c) return B2M_ERR_NOT_INITIALIZED;

@@ -46,12 +46,32 @@ struct LookbackSlot {
 uint64_t workspace_bytes_for(int logn);
 uint64_t carry_scratch_bytes(int logn);
 
+// Optional tracing of a launch sequence: an event is recorded on the stream
+// before every kernel and once after the last one.
+struct Tracer {
+    static constexpr int CAP = 16;
+    cudaEvent_t ev[CAP + 1];
+    uint32_t kind[CAP], logr[CAP];
+    int n = 0;
+    void mark(cudaStream_t s, uint32_t k, uint32_t r) {
+        if (n < CAP) {
+            kind[n] = k;
+            logr[n] = r;
+            cudaEventRecord(ev[n], s);
+            ++n;
+        }
+    }
+    void end(cudaStream_t s) { cudaEventRecord(ev[n], s); }
+};
+
 // Kernel launch sequence for one product on `stream`.
 //   a, b: device limbs; out: na+nb limbs; out_len: device u64 (may be null).
 //   ws: workspace of workspace_bytes_for(logn) bytes; err: device error word.
 cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb, u32* out,
                            uint64_t* out_len, void* ws, const Plan& plan, const RootTables& tw,
-                           u32* err, cudaStream_t stream);
+                           u32* err, cudaStream_t stream, Tracer* tr = nullptr);
+// Kernels one product launches under plan p.
+int plan_launches(const Plan& p);
 
 // One-time per-device kernel attribute setup (dynamic shared memory limits).
 cudaError_t configure_kernels();

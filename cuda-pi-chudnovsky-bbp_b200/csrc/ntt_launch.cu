@@ -15,6 +15,7 @@
 // (include/ntt.h:70-91) -- all replaced by the sequence below.
 #include <cuda_runtime.h>
 
+#include "b2m.h"
 #include "b2m_internal.h"
 #include "carry.cuh"
 
@@ -90,19 +91,26 @@ cudaError_t configure_kernels() {
     return e;
 }
 
+int plan_launches(const Plan& p) { return p.npass == 0 ? 1 : 3 * p.npass; }
+
 static cudaError_t launch_forward(const u32* limbs, uint64_t nlimbs, u64* buf, const Plan& p,
                                   const RootTables& tw, bool fused, const u64* aspec, u64 ninv,
-                                  cudaStream_t s) {
+                                  cudaStream_t s, Tracer* tr) {
+    if (tr) tr->mark(s, B2M_K_FWD_FIRST, p.logr[0]);
     cudaError_t e = launch_fwd_first(p.logr[0], pass_geo(p, 0), s, limbs, 2 * nlimbs, buf, tw);
-    for (int k = 1; e == cudaSuccess && k + 1 < p.npass; ++k) e = launch_fwd_mid(p.logr[k], pass_geo(p, k), s, buf, tw);
+    for (int k = 1; e == cudaSuccess && k + 1 < p.npass; ++k) {
+        if (tr) tr->mark(s, B2M_K_FWD_MID, p.logr[k]);
+        e = launch_fwd_mid(p.logr[k], pass_geo(p, k), s, buf, tw);
+    }
     if (e != cudaSuccess) return e;
     const int last = p.npass - 1;
+    if (tr) tr->mark(s, fused ? B2M_K_FUSED_LAST : B2M_K_FWD_LAST, p.logr[last]);
     return fused ? launch_fused_last(p.logr[last], pass_geo(p, last), s, buf, aspec, ninv, tw)
                  : launch_fwd_last(p.logr[last], pass_geo(p, last), s, buf, tw);
 }
 
 cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb, u32* out, uint64_t* out_len,
-                           void* ws, const Plan& p, const RootTables& tw, u32* err, cudaStream_t s) {
+                           void* ws, const Plan& p, const RootTables& tw, u32* err, cudaStream_t s, Tracer* tr) {
     const int logn = p.logn;
     const u64 ninv = gl_inv(1ull << logn);
     const u64 nout = na + nb;
@@ -113,8 +121,11 @@ cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb,
         g.grid = 1;
         g.block = (unsigned)T;
         g.smem = 2 * rp * sizeof(u64) + (size_t)T * 2 * sizeof(u64);
-        return launch_mul_small(logn, g, s, a, na, b, nb, out, nout,
-                                reinterpret_cast<unsigned long long*>(out_len), ninv, tw);
+        if (tr) tr->mark(s, B2M_K_SMALL, logn);
+        cudaError_t e = launch_mul_small(logn, g, s, a, na, b, nb, out, nout,
+                                         reinterpret_cast<unsigned long long*>(out_len), ninv, tw);
+        if (tr) tr->end(s);
+        return e;
     }
     const uint64_t n = 1ull << logn;
     u64* bufA = static_cast<u64*>(ws);
@@ -129,11 +140,16 @@ cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb,
     unsigned long long* ol = out_len ? reinterpret_cast<unsigned long long*>(out_len) : len_tmp;
     if (out_len && (e = cudaMemsetAsync(out_len, 0, sizeof(uint64_t), s)) != cudaSuccess) return e;
 
-    if ((e = launch_forward(a, na, bufA, p, tw, false, nullptr, 0, s)) != cudaSuccess) return e;
-    if ((e = launch_forward(b, nb, bufB, p, tw, true, bufA, ninv, s)) != cudaSuccess) return e;
-    for (int k = p.npass - 2; k >= 0; --k)
+    if ((e = launch_forward(a, na, bufA, p, tw, false, nullptr, 0, s, tr)) != cudaSuccess) return e;
+    if ((e = launch_forward(b, nb, bufB, p, tw, true, bufA, ninv, s, tr)) != cudaSuccess) return e;
+    for (int k = p.npass - 2; k >= 0; --k) {
+        if (tr) tr->mark(s, B2M_K_INV_MID, p.logr[k]);
         if ((e = launch_inv_mid(p.logr[k], pass_geo(p, k), s, bufB, tw)) != cudaSuccess) return e;
-    return launch_carry((unsigned)nchunks, s, bufB, out, nout, slots, ticket, ol, err);
+    }
+    if (tr) tr->mark(s, B2M_K_CARRY, 0);
+    e = launch_carry((unsigned)nchunks, s, bufB, out, nout, slots, ticket, ol, err);
+    if (tr) tr->end(s);
+    return e;
 }
 
 }  // namespace b2m

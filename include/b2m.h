@@ -103,6 +103,45 @@ b2m_status b2m_mul_device(const uint32_t* d_a, uint64_t na, const uint32_t* d_b,
  * raised by this library's kernels since the last check. */
 b2m_status b2m_stream_check(b2m_stream stream);
 
+/* ---- plan inspection and tracing -------------------------------------------- */
+
+/* Kernel kinds of a product's launch sequence. */
+enum {
+    B2M_K_FWD_FIRST = 1,   /* first forward pass: u32 limbs -> 16-bit digits -> pass 1 */
+    B2M_K_FWD_MID = 2,     /* a middle forward pass */
+    B2M_K_FWD_LAST = 3,    /* operand A's last forward pass */
+    B2M_K_FUSED_LAST = 4,  /* operand B's last forward pass + pointwise + first inverse pass */
+    B2M_K_INV_MID = 5,     /* an inverse pass (pass 1 yields the coefficients) */
+    B2M_K_CARRY = 6,       /* decoupled-lookback carry into u32 limbs */
+    B2M_K_SMALL = 7        /* whole product in one CTA (transform length <= 2^13) */
+};
+
+typedef struct b2m_plan_desc {
+    uint32_t ntt_log2;      /* log2 of the transform length */
+    uint32_t npass;         /* 0 = single-CTA product, else 2 or 3 passes */
+    uint32_t logr[3];       /* radix exponent of each pass */
+    uint32_t logc[3];       /* columns per CTA (log2) of each pass */
+    uint32_t launches;      /* kernels launched per product */
+} b2m_plan_desc;
+
+/* Describes the transform plan the library uses for an na x nb product (no
+ * reference counterpart: the reference always runs radix-2 stages). */
+b2m_status b2m_plan_describe(uint64_t na, uint64_t nb, b2m_plan_desc* desc);
+
+typedef struct b2m_kernel_time {
+    uint32_t kind;          /* B2M_K_* */
+    uint32_t logr;          /* pass radix exponent (0 for carry) */
+    float ms;               /* device time of that launch, CUDA events on the stream */
+} b2m_kernel_time;
+
+/* b2m_mul_device with a CUDA event recorded around every kernel launch on
+ * `stream`; synchronises and returns the per-launch device times in launch
+ * order (at most cap entries, *n receives the count). For tracing and the
+ * benchmark's roofline figures; the product is identical to b2m_mul_device. */
+b2m_status b2m_mul_device_traced(const uint32_t* d_a, uint64_t na, const uint32_t* d_b, uint64_t nb,
+                                 uint32_t* d_out, uint64_t out_cap, uint64_t* d_out_len,
+                                 b2m_stream stream, b2m_kernel_time* times, uint32_t cap, uint32_t* n);
+
 #ifdef __cplusplus
 }
 #endif
