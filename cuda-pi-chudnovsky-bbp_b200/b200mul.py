@@ -66,6 +66,8 @@ _sig("b2m_mul_host", ctypes.c_int, [_u32p, _u64, _u32p, _u64, _u32p, _u64, _u64p
 _sig("b2m_mul_device", ctypes.c_int,
      [ctypes.c_void_p, _u64, ctypes.c_void_p, _u64, ctypes.c_void_p, _u64, ctypes.c_void_p, ctypes.c_void_p])
 _sig("b2m_stream_check", ctypes.c_int, [ctypes.c_void_p])
+_sig("b2m_mul_device_noalloc", ctypes.c_int,
+     [ctypes.c_void_p, _u64, ctypes.c_void_p, _u64, ctypes.c_void_p, _u64, ctypes.c_void_p, ctypes.c_void_p])
 
 
 class PlanDesc(ctypes.Structure):
@@ -142,6 +144,15 @@ def mul_device(a_ptr: int, na: int, b_ptr: int, nb: int, out_ptr: int, out_cap: 
     """Device-pointer product ordered on `stream` (raw CUDA handles as ints)."""
     check(lib.b2m_mul_device(a_ptr, na, b_ptr, nb, out_ptr, out_cap, out_len_ptr or None, stream or None),
           "b2m_mul_device")
+
+
+def mul_device_noalloc(a_ptr: int, na: int, b_ptr: int, nb: int, out_ptr: int, out_cap: int,
+                       out_len_ptr: int = 0, stream: int = 0) -> None:
+    """The product without any device allocation, for callers that cannot
+    allocate at call time: scratch is the library's fixed static device array,
+    so na + nb <= 2^19 limbs, and calls that overlap on the GPU race."""
+    check(lib.b2m_mul_device_noalloc(a_ptr, na, b_ptr, nb, out_ptr, out_cap, out_len_ptr or None,
+                                     stream or None), "b2m_mul_device_noalloc")
 
 
 def stream_check(stream: int = 0) -> None:

@@ -47,13 +47,14 @@ GL_FN u64 gl_mulhi(u64 a, u64 b) {
 // materialised as 0 or 0xFFFFFFFF (= EPS), is what gets subtracted.
 GL_FN u64 gl_sub(u64 a, u64 b) {
 #if defined(__CUDA_ARCH__)
-    u32 d0, d1, m;
-    asm("sub.cc.u32 %0, %3, %5;\n\t"
-        "subc.cc.u32 %1, %4, %6;\n\t"
-        "subc.u32 %2, 0, 0;\n\t"
-        "sub.cc.u32 %0, %0, %2;\n\t"
-        "subc.u32 %1, %1, 0;\n\t"
-        : "=r"(d0), "=r"(d1), "=r"(m)
+    u32 d0, d1;
+    asm("{\n\t.reg .u32 m;\n\t"
+        "sub.cc.u32 %0, %2, %4;\n\t"
+        "subc.cc.u32 %1, %3, %5;\n\t"
+        "subc.u32 m, 0, 0;\n\t"
+        "sub.cc.u32 %0, %0, m;\n\t"
+        "subc.u32 %1, %1, 0;\n\t}"
+        : "=r"(d0), "=r"(d1)
         : "r"((u32)a), "r"((u32)(a >> 32)), "r"((u32)b), "r"((u32)(b >> 32)));
     return ((u64)d1 << 32) | d0;
 #else

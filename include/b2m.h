@@ -99,6 +99,23 @@ b2m_status b2m_mul_device(const uint32_t* d_a, uint64_t na, const uint32_t* d_b,
                           uint32_t* d_out, uint64_t out_cap, uint64_t* d_out_len,
                           b2m_stream stream);
 
+/* No counterpart in the reference. The same product as b2m_mul_device, for
+ * callers that cannot allocate device memory when they multiply (their HBM is
+ * owned by another allocator, or a cudaMalloc's device-wide synchronisation
+ * and latency are not acceptable in their loop): it allocates nothing. Its
+ * scratch is one fixed static device array of about 16 MiB, present on every
+ * GPU that loads the library until the process exits, so it accepts
+ * transform lengths up to 2^20 only (na + nb <= 2^19 limbs) and returns
+ * B2M_ERR_TOO_LARGE beyond that. Every call shares that array: calls whose
+ * device work overlaps (other streams, other host threads) race, and the
+ * caller must serialise them. The first call on a device looks up the
+ * array's device address; make that first call before any stream capture.
+ * Inputs, output and *d_out_len are the caller's device buffers, as for
+ * b2m_mul_device. */
+b2m_status b2m_mul_device_noalloc(const uint32_t* d_a, uint64_t na, const uint32_t* d_b, uint64_t nb,
+                                  uint32_t* d_out, uint64_t out_cap, uint64_t* d_out_len,
+                                  b2m_stream stream);
+
 /* Synchronises `stream` and reports (and clears) any device-side failure
  * raised by this library's kernels since the last check. */
 b2m_status b2m_stream_check(b2m_stream stream);
