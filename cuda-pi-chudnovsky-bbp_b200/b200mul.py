@@ -195,3 +195,54 @@ def mul_device_traced(a_ptr: int, na: int, b_ptr: int, nb: int, out_ptr: int, ou
     check(lib.b2m_mul_device_traced(a_ptr, na, b_ptr, nb, out_ptr, out_cap, out_len_ptr or None, stream or None,
                                     times, 16, ctypes.byref(n)), "b2m_mul_device_traced")
     return [(KERNEL_KINDS[times[i].kind], times[i].logr, times[i].ms) for i in range(n.value)]
+
+
+# ---- batched products ----------------------------------------------------------------
+class Job(ctypes.Structure):
+    """b2m_job: device pointers of one product of a batch."""
+    _fields_ = [("a", ctypes.c_void_p), ("na", _u64), ("b", ctypes.c_void_p), ("nb", _u64),
+                ("out", ctypes.c_void_p), ("out_cap", _u64), ("out_len", ctypes.c_void_p)]
+
+
+BATCH_GRAPH, BATCH_AUTOTUNE = 1, 2
+_sig("b2m_batch_create", ctypes.c_int, [ctypes.POINTER(Job), _u64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p)])
+_sig("b2m_batch_launch", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p])
+_sig("b2m_batch_destroy", ctypes.c_int, [ctypes.c_void_p])
+_sig("b2m_mul_batch", ctypes.c_int, [ctypes.POINTER(Job), _u64, ctypes.c_void_p])
+
+
+def _jobs(jobs):
+    arr = (Job * max(1, len(jobs)))()
+    for i, (a, na, b, nb, out, cap, olen) in enumerate(jobs):
+        arr[i] = Job(a or None, na, b or None, nb, out or None, cap, olen or None)
+    return arr
+
+
+class Batch:
+    """A planned batch of independent products (device pointers); launch() it
+    any number of times. jobs: [(a_ptr, na, b_ptr, nb, out_ptr, out_cap, out_len_ptr)]."""
+
+    def __init__(self, jobs, flags: int = BATCH_GRAPH):
+        self._arr = _jobs(jobs)
+        self.handle = ctypes.c_void_p()
+        check(lib.b2m_batch_create(self._arr, len(jobs), flags, ctypes.byref(self.handle)), "b2m_batch_create")
+
+    def launch(self, stream: int = 0) -> None:
+        check(lib.b2m_batch_launch(self.handle, stream or None), "b2m_batch_launch")
+
+    def close(self) -> None:
+        if self.handle:
+            check(lib.b2m_batch_destroy(self.handle), "b2m_batch_destroy")
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def mul_batch(jobs, stream: int = 0) -> None:
+    """One-shot batch (no graph), synchronous on `stream`."""
+    arr = _jobs(jobs)
+    check(lib.b2m_mul_batch(arr, len(jobs), stream or None), "b2m_mul_batch")

@@ -23,6 +23,12 @@ struct Context {
     std::mutex host_mu;                  // serialises b2m_mul_host (shared buffers)
     void* host_dev = nullptr;            // device buffers of b2m_mul_host, grown on demand
     uint64_t host_dev_cap = 0;
+    // Autotuned plans of batched buckets per transform length (-1: default).
+    int tuned_r0[MAX_LOGN + 1];
+    int tuned_tile[MAX_LOGN + 1];
+    Context() {
+        for (int i = 0; i <= MAX_LOGN; ++i) tuned_r0[i] = tuned_tile[i] = -1;
+    }
 };
 
 extern Context* g_ctx;

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 #include "gl.cuh"
 
@@ -36,6 +37,8 @@ struct Plan {
 };
 
 Plan make_plan(int logn);
+Plan make_plan_custom(int logn, int r0, int tile);
+std::vector<Plan> plan_candidates(int logn);
 
 // Per-product workspace layout (bytes): two N-element u64 arrays plus the
 // carry scratch (lookback slots, ticket, out_len staging).
@@ -44,6 +47,21 @@ struct LookbackSlot {
     u32 flag, pad;
 };
 uint64_t workspace_bytes_for(int logn);
+
+// One product's device pointers. Batched launches give kernels a table of
+// these and each CTA reads jobs[blockIdx.y] (blockIdx.x for the single-CTA
+// kernel); single products pass a null table and plain arguments.
+struct ProdJob {
+    const u32* a;
+    const u32* b;
+    u32* out;
+    unsigned long long* out_len;  // may be null
+    u64 na, nb;
+    u64* bufA;                    // transform buffers of N elements each
+    u64* bufB;
+    LookbackSlot* slots;          // carry scratch: N / CARRY_CHUNK slots + ticket
+    u32* ticket;
+};
 uint64_t carry_scratch_bytes(int logn);
 
 // Optional tracing of a launch sequence: an event is recorded on the stream
@@ -67,6 +85,11 @@ struct Tracer {
 // Kernel launch sequence for one product on `stream`.
 //   a, b: device limbs; out: na+nb limbs; out_len: device u64 (may be null).
 //   ws: workspace of workspace_bytes_for(logn) bytes; err: device error word.
+// All passes, the carry and the bookkeeping of one size bucket of a batch:
+// `njobs` products of plan p whose pointers are in the device table `jobs`.
+cudaError_t launch_bucket(const Plan& p, const ProdJob* jobs, unsigned njobs, const RootTables& tw, u32* err,
+                          cudaStream_t s);
+
 cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb, u32* out,
                            uint64_t* out_len, void* ws, const Plan& plan, const RootTables& tw,
                            u32* err, cudaStream_t stream, Tracer* tr = nullptr);
@@ -86,17 +109,25 @@ PassGeo pass_geo(const Plan& p, int k);
 
 // Per-family launchers (ntt_fam_*.cu, ntt_carry.cu); each dispatches on the
 // radix exponent to the matching template instantiation.
+// `jobs` (device table, may be null) and `njobs` select batched launches:
+// grid.y (grid.x for the single-CTA kernel) runs over the jobs.
 cudaError_t launch_fwd_first(int logr, const PassGeo& g, cudaStream_t s, const u32* limbs, u64 ndig, u64* out,
-                             const RootTables& tw);
-cudaError_t launch_fwd_mid(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw);
-cudaError_t launch_inv_mid(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw);
-cudaError_t launch_fwd_last(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw);
+                             const RootTables& tw, const ProdJob* jobs = nullptr, unsigned njobs = 1,
+                             int operand = 0);
+cudaError_t launch_fwd_mid(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw,
+                           const ProdJob* jobs = nullptr, unsigned njobs = 1, int operand = 0);
+cudaError_t launch_inv_mid(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw,
+                           const ProdJob* jobs = nullptr, unsigned njobs = 1);
+cudaError_t launch_fwd_last(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw,
+                            const ProdJob* jobs = nullptr, unsigned njobs = 1);
 cudaError_t launch_fused_last(int logr, const PassGeo& g, cudaStream_t s, u64* bbuf, const u64* aspec, u64 ninv,
-                              const RootTables& tw);
+                              const RootTables& tw, const ProdJob* jobs = nullptr, unsigned njobs = 1);
 cudaError_t launch_mul_small(int logn, const PassGeo& g, cudaStream_t s, const u32* a, u64 na, const u32* b, u64 nb,
-                             u32* out, u64 nout, unsigned long long* out_len, u64 ninv, const RootTables& tw);
+                             u32* out, u64 nout, unsigned long long* out_len, u64 ninv, const RootTables& tw,
+                             const ProdJob* jobs = nullptr, unsigned njobs = 1);
 cudaError_t launch_carry(unsigned nchunks, cudaStream_t s, const u64* coef, u32* out, u64 nout,
-                         LookbackSlot* slots, u32* ticket, unsigned long long* out_len, u32* err);
+                         LookbackSlot* slots, u32* ticket, unsigned long long* out_len, u32* err,
+                         const ProdJob* jobs = nullptr, unsigned njobs = 1);
 cudaError_t configure_first();
 cudaError_t configure_mid();
 cudaError_t configure_last();

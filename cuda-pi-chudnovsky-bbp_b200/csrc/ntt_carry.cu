@@ -31,7 +31,17 @@ constexpr int LOOKBACK_SPIN_LIMIT = 1 << 22;
 
 __global__ void __launch_bounds__(CARRY_THREADS) k_carry(const u64* __restrict__ coef, u32* __restrict__ out,
                                                          u64 nout, LookbackSlot* slots, u32* ticket,
-                                                         unsigned long long* out_len, u32* err) {
+                                                         unsigned long long* out_len, u32* err,
+                                                         const ProdJob* __restrict__ jobs) {
+    if (jobs) {
+        const ProdJob& J = jobs[blockIdx.y];
+        coef = J.bufB;
+        out = J.out;
+        nout = J.na + J.nb;
+        slots = J.slots;
+        ticket = J.ticket;
+        out_len = J.out_len;
+    }
     __shared__ u32 s_chunk;
     __shared__ u64 s_cin;
     __shared__ CState s_ws[CARRY_THREADS / 32 + 1];
@@ -126,8 +136,9 @@ __global__ void __launch_bounds__(CARRY_THREADS) k_carry(const u64* __restrict__
 
 
 cudaError_t launch_carry(unsigned nchunks, cudaStream_t s, const u64* coef, u32* out, u64 nout,
-                         LookbackSlot* slots, u32* ticket, unsigned long long* out_len, u32* err) {
-    k_carry<<<nchunks, CARRY_THREADS, 0, s>>>(coef, out, nout, slots, ticket, out_len, err);
+                         LookbackSlot* slots, u32* ticket, unsigned long long* out_len, u32* err,
+                         const ProdJob* jobs, unsigned njobs) {
+    k_carry<<<dim3(nchunks, njobs), CARRY_THREADS, 0, s>>>(coef, out, nout, slots, ticket, out_len, err, jobs);
     return cudaGetLastError();
 }
 

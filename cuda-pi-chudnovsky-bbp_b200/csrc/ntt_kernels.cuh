@@ -59,8 +59,15 @@ __device__ __forceinline__ u64 digit_of(const u32* __restrict__ limbs, u64 ndig,
 template <int LOGR>
 __global__ void __launch_bounds__(PASS_THREADS_MAX) k_fwd_first(const u32* __restrict__ limbs, u64 ndig,
                                                                 u64* __restrict__ out, int logS, int logC,
-                                                                int logM, RootTables tw) {
+                                                                int logM, RootTables tw,
+                                                                const ProdJob* __restrict__ jobs, int operand) {
     extern __shared__ u64 sm[];
+    if (jobs) {
+        const ProdJob& J = jobs[blockIdx.y];
+        limbs = operand ? J.b : J.a;
+        ndig = 2 * (operand ? J.nb : J.na);
+        out = operand ? J.bufB : J.bufA;
+    }
     const Tile<LOGR, MAP_COL> tl{logC};
     const u64 g0 = (u64)blockIdx.x << logC;
     const int cm = (1 << logC) - 1, total = (1 << LOGR) << logC;
@@ -84,8 +91,10 @@ __global__ void __launch_bounds__(PASS_THREADS_MAX) k_fwd_first(const u32* __res
 // A later, not-last forward pass, in place.
 template <int LOGR>
 __global__ void __launch_bounds__(PASS_THREADS_MAX) k_fwd_mid(u64* __restrict__ buf, int logS, int logC, int logM,
-                                                              RootTables tw) {
+                                                              RootTables tw, const ProdJob* __restrict__ jobs,
+                                                              int operand) {
     extern __shared__ u64 sm[];
+    if (jobs) buf = operand ? jobs[blockIdx.y].bufB : jobs[blockIdx.y].bufA;
     const Tile<LOGR, MAP_COL> tl{logC};
     const u64 g0 = (u64)blockIdx.x << logC;
     const int cm = (1 << logC) - 1, total = (1 << LOGR) << logC;
@@ -111,8 +120,9 @@ __global__ void __launch_bounds__(PASS_THREADS_MAX) k_fwd_mid(u64* __restrict__ 
 // coefficients (N^-1 already applied) in natural order.
 template <int LOGR>
 __global__ void __launch_bounds__(PASS_THREADS_MAX) k_inv_mid(u64* __restrict__ buf, int logS, int logC, int logM,
-                                                              RootTables tw) {
+                                                              RootTables tw, const ProdJob* __restrict__ jobs) {
     extern __shared__ u64 sm[];
+    if (jobs) buf = jobs[blockIdx.y].bufB;
     const Tile<LOGR, MAP_COL> tl{logC};
     const u64 g0 = (u64)blockIdx.x << logC;
     const int cm = (1 << logC) - 1, total = (1 << LOGR) << logC;
@@ -136,8 +146,10 @@ __global__ void __launch_bounds__(PASS_THREADS_MAX) k_inv_mid(u64* __restrict__ 
 // Last forward pass of operand A (S = 1: each column is a contiguous
 // sub-problem, so the CTA's tile is one contiguous range of R*C elements).
 template <int LOGR>
-__global__ void __launch_bounds__(PASS_THREADS_MAX) k_fwd_last(u64* __restrict__ buf, int logC, RootTables tw) {
+__global__ void __launch_bounds__(PASS_THREADS_MAX) k_fwd_last(u64* __restrict__ buf, int logC, RootTables tw,
+                                                               const ProdJob* __restrict__ jobs) {
     extern __shared__ u64 sm[];
+    if (jobs) buf = jobs[blockIdx.y].bufA;
     const Tile<LOGR, MAP_ROW> tl{logC};
     u64* base = buf + ((u64)blockIdx.x << (LOGR + logC));
     const int total = (1 << LOGR) << logC;
@@ -153,8 +165,13 @@ __global__ void __launch_bounds__(PASS_THREADS_MAX) k_fwd_last(u64* __restrict__
 // positions) and N^-1, then the first inverse pass -- one tile, one kernel.
 template <int LOGR>
 __global__ void __launch_bounds__(PASS_THREADS_MAX) k_fused_last(u64* __restrict__ bbuf, const u64* __restrict__ aspec,
-                                                                 int logC, u64 ninv, RootTables tw) {
+                                                                 int logC, u64 ninv, RootTables tw,
+                                                                 const ProdJob* __restrict__ jobs) {
     extern __shared__ u64 sm[];
+    if (jobs) {
+        bbuf = jobs[blockIdx.y].bufB;
+        aspec = jobs[blockIdx.y].bufA;
+    }
     const Tile<LOGR, MAP_ROW> tl{logC};
     const u64 off = (u64)blockIdx.x << (LOGR + logC);
     u64* base = bbuf + off;
@@ -182,7 +199,18 @@ __global__ void __launch_bounds__(PASS_THREADS_MAX) k_fused_last(u64* __restrict
 template <int LOGN>
 __global__ void __launch_bounds__(512) k_mul_small(const u32* __restrict__ a, u64 na, const u32* __restrict__ b,
                                                    u64 nb, u32* __restrict__ out, u64 nout,
-                                                   unsigned long long* out_len, u64 ninv, RootTables tw) {
+                                                   unsigned long long* out_len, u64 ninv, RootTables tw,
+                                                   const ProdJob* __restrict__ jobs) {
+    if (jobs) {
+        const ProdJob& J = jobs[blockIdx.x];
+        a = J.a;
+        b = J.b;
+        na = J.na;
+        nb = J.nb;
+        out = J.out;
+        nout = J.na + J.nb;
+        out_len = J.out_len;
+    }
     using TL = Tile<LOGN, MAP_ROW>;
     constexpr int N = 1 << LOGN, RP = TL::RP, G = N < 16 ? N : 16;
     extern __shared__ u64 sm[];

@@ -15,13 +15,20 @@
 // (include/ntt.h:70-91) -- all replaced by the sequence below.
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "b2m.h"
 #include "b2m_internal.h"
 #include "carry.cuh"
 
 namespace b2m {
 
-Plan make_plan(int logn) {
+Plan make_plan(int logn) { return make_plan_custom(logn, -1, -1); }
+
+// r0 < 0 / tile < 0 pick the defaults: two passes up to 2^26, the first pass
+// keeping at least 4 columns (32-byte rows) in a 2^14-element tile and the
+// last (contiguous) pass taking up to 2^14; three passes above.
+Plan make_plan_custom(int logn, int r0, int tile) {
     Plan p;
     p.logn = logn;
     if (logn <= SMALL_MAX_LOGN) {
@@ -29,10 +36,8 @@ Plan make_plan(int logn) {
         return p;
     }
     if (logn <= 26) {
-        // Two passes; the first keeps at least 4 columns (32-byte rows) in a
-        // 2^14-element tile, the last (contiguous) pass takes up to 2^14.
         p.npass = 2;
-        p.logr[0] = logn / 2 < 12 ? logn / 2 : 12;
+        p.logr[0] = r0 > 0 ? r0 : (logn / 2 < 12 ? logn / 2 : 12);
         p.logr[1] = logn - p.logr[0];
     } else {
         p.npass = 3;
@@ -40,7 +45,7 @@ Plan make_plan(int logn) {
         p.logr[1] = logn / 3;
         p.logr[2] = logn - 2 * (logn / 3);
     }
-    const int tile = logn >= 20 ? 14 : (logn >= 17 ? 13 : 12);
+    if (tile <= 0) tile = logn >= 20 ? 14 : (logn >= 17 ? 13 : 12);
     int before = 0;
     for (int k = 0; k < p.npass; ++k) {
         const int r = p.logr[k];
@@ -53,6 +58,23 @@ Plan make_plan(int logn) {
         before += r;
     }
     return p;
+}
+
+std::vector<Plan> plan_candidates(int logn) {
+    std::vector<Plan> v;
+    if (logn <= SMALL_MAX_LOGN || logn > 26) {
+        v.push_back(make_plan(logn));
+        return v;
+    }
+    for (int r0 = 7; r0 <= 12; ++r0) {
+        const int r1 = logn - r0;
+        if (r1 < 7 || r1 > 14) continue;
+        for (int tile = 12; tile <= 14; ++tile) {
+            if (r1 > tile && tile < 14) continue;  // last pass needs its whole column in the tile
+            v.push_back(make_plan_custom(logn, r0, tile));
+        }
+    }
+    return v;
 }
 
 PassGeo pass_geo(const Plan& p, int k) {
@@ -150,6 +172,36 @@ cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb,
     e = launch_carry((unsigned)nchunks, s, bufB, out, nout, slots, ticket, ol, err);
     if (tr) tr->end(s);
     return e;
+}
+
+cudaError_t launch_bucket(const Plan& p, const ProdJob* jobs, unsigned njobs, const RootTables& tw, u32* err,
+                          cudaStream_t s) {
+    const int logn = p.logn;
+    const u64 ninv = gl_inv(1ull << logn);
+    if (p.npass == 0) {
+        PassGeo g{};
+        const int T = logn >= 4 ? (1 << (logn - 4)) : 1;
+        const size_t rp = (size_t)(1 << logn) + (size_t)((1 << logn) >> 6);
+        g.grid = 1;
+        g.block = (unsigned)T;
+        g.smem = 2 * rp * sizeof(u64) + (size_t)T * 2 * sizeof(u64);
+        return launch_mul_small(logn, g, s, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, ninv, tw, jobs, njobs);
+    }
+    cudaError_t e = cudaSuccess;
+    for (int op = 0; op < 2 && e == cudaSuccess; ++op) {
+        e = launch_fwd_first(p.logr[0], pass_geo(p, 0), s, nullptr, 0, nullptr, tw, jobs, njobs, op);
+        for (int k = 1; e == cudaSuccess && k + 1 < p.npass; ++k)
+            e = launch_fwd_mid(p.logr[k], pass_geo(p, k), s, nullptr, tw, jobs, njobs, op);
+        if (e != cudaSuccess) break;
+        const int last = p.npass - 1;
+        e = op == 0 ? launch_fwd_last(p.logr[last], pass_geo(p, last), s, nullptr, tw, jobs, njobs)
+                    : launch_fused_last(p.logr[last], pass_geo(p, last), s, nullptr, nullptr, ninv, tw, jobs, njobs);
+    }
+    for (int k = p.npass - 2; e == cudaSuccess && k >= 0; --k)
+        e = launch_inv_mid(p.logr[k], pass_geo(p, k), s, nullptr, tw, jobs, njobs);
+    if (e != cudaSuccess) return e;
+    const unsigned nchunks = (unsigned)((1ull << logn) / CARRY_CHUNK);
+    return launch_carry(nchunks, s, nullptr, nullptr, 0, nullptr, nullptr, nullptr, err, jobs, njobs);
 }
 
 }  // namespace b2m

@@ -120,6 +120,47 @@ b2m_status b2m_mul_device_noalloc(const uint32_t* d_a, uint64_t na, const uint32
  * raised by this library's kernels since the last check. */
 b2m_status b2m_stream_check(b2m_stream stream);
 
+/* ---- batched products ---------------------------------------------------------
+ * No counterpart in the reference, whose tree (src/chudnovsky.cpp:64-102)
+ * multiplies one pair at a time, each call paying its own allocation, copies
+ * and radix-2 launches. A batch runs many independent products of mixed sizes
+ * together: jobs are bucketed by transform length, every bucket runs as one
+ * set of launches covering all of its products (grid dimension over the
+ * jobs), buckets run concurrently on forked streams, and the whole sequence
+ * can be captured once into a CUDA graph and replayed. */
+
+typedef struct b2m_job {
+    const uint32_t* a;     /* device limbs */
+    uint64_t na;
+    const uint32_t* b;
+    uint64_t nb;
+    uint32_t* out;         /* device, out_cap >= na + nb limbs */
+    uint64_t out_cap;
+    uint64_t* out_len;     /* device pointer or NULL: trimmed product length */
+} b2m_job;
+
+typedef struct b2m_batch b2m_batch;
+
+#define B2M_BATCH_GRAPH 1u     /* capture the launch sequence into a CUDA graph */
+#define B2M_BATCH_AUTOTUNE 2u  /* time candidate pass splits and tile sizes per size
+                                  bucket at creation and keep the fastest */
+
+/* Plans a batch over `jobs` (copied; the device buffers they point to must
+ * stay valid while the batch exists). Allocates the batch's workspace from
+ * the HBM budget. The batch can be launched any number of times; each launch
+ * recomputes every product from the current contents of the inputs. */
+b2m_status b2m_batch_create(const b2m_job* jobs, uint64_t njobs, uint32_t flags, b2m_batch** batch);
+
+/* Enqueues every product of the batch on `stream` (one graph launch when
+ * created with B2M_BATCH_GRAPH). Launches of one batch must not overlap. */
+b2m_status b2m_batch_launch(b2m_batch* batch, b2m_stream stream);
+
+/* Releases the batch (after synchronising its last launch). */
+b2m_status b2m_batch_destroy(b2m_batch* batch);
+
+/* create + launch + destroy without a graph: for one-shot batches. */
+b2m_status b2m_mul_batch(const b2m_job* jobs, uint64_t njobs, b2m_stream stream);
+
 /* ---- plan inspection and tracing -------------------------------------------- */
 
 /* Kernel kinds of a product's launch sequence. */
