@@ -363,12 +363,129 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+def batch_sizes(n: int, seed: int):
+    """n pairs, na and nb independently log-uniform over [64, 65536] limbs:
+    floor(2^(6 + 10u)) with u uniform in [0, 1)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    u = rng.random((n, 2))
+    return [(int(2 ** (6 + 10 * x)), int(2 ** (6 + 10 * y))) for x, y in u]
+
+
+def run_batch(args) -> None:
+    """Batched uneven products: 4096 log-uniform pairs in one graph launch
+    versus one b2m_mul_device call per product on the same GPU."""
+    import numpy as np
+    import torch
+
+    import b200mul
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    b200mul.init(local)
+    sizes = batch_sizes(args.batch_jobs, 4096 + rank)
+    total_limbs = sum(a + b for a, b in sizes)
+    # Operands packed into one device tensor, outputs into two (batched, single).
+    offs, tot = [], 0
+    for na, nb in sizes:
+        offs.append((tot, tot + na + 64))
+        tot += na + nb + 128
+    host = np.zeros(tot, np.uint32)
+    for i, ((na, nb), (oa, ob)) in enumerate(zip(sizes, offs)):
+        host[oa:oa + na] = b200mul.gen_operand(7 * i + 1, na)
+        host[ob:ob + nb] = b200mul.gen_operand(7 * i + 2, nb)
+    dev = torch.from_numpy(host.view(np.int32)).cuda()
+    out1 = torch.zeros(tot, dtype=torch.int32, device="cuda")
+    out2 = torch.zeros(tot, dtype=torch.int32, device="cuda")
+    len1 = torch.zeros(len(sizes), dtype=torch.int64, device="cuda")
+    len2 = torch.zeros(len(sizes), dtype=torch.int64, device="cuda")
+    base = dev.data_ptr()
+    jobs = [(base + 4 * oa, na, base + 4 * ob, nb, out1.data_ptr() + 4 * oa, na + nb, len1.data_ptr() + 8 * i)
+            for i, ((na, nb), (oa, ob)) in enumerate(zip(sizes, offs))]
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    t0 = time.perf_counter()
+    bt = b200mul.Batch(jobs, b200mul.BATCH_GRAPH | b200mul.BATCH_AUTOTUNE)
+    plan_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        bt.launch(sp)
+    b200mul.stream_check(sp)
+
+    def timed(fn, reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    batched_ms = timed(lambda: bt.launch(sp), args.steps)
+    clocks = sampler.stop()
+
+    def one_at_a_time():
+        for i, ((na, nb), (oa, ob)) in enumerate(zip(sizes, offs)):
+            b200mul.mul_device(base + 4 * oa, na, base + 4 * ob, nb, out2.data_ptr() + 4 * oa, na + nb,
+                               len2.data_ptr() + 8 * i, sp)
+
+    one_at_a_time()
+    single_ms = timed(one_at_a_time, max(1, min(3, args.steps)))
+    b200mul.stream_check(sp)
+    same = bool(torch.equal(out1, out2) and torch.equal(len1, len2))
+    bt.close()
+    if not same:
+        raise RuntimeError("batched and one-at-a-time products differ")
+    if dist is not None:
+        t = torch.tensor([batched_ms, single_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        batched_ms, single_ms = (float(x) for x in t.tolist())
+    if rank == 0:
+        gl_b = total_limbs * world / (batched_ms * 1e-3) / 1e9
+        gl_s = total_limbs * world / (single_ms * 1e-3) / 1e9
+        print(json.dumps({
+            "metric": "batched Glimbs/s (4096 log-uniform pairs, 64..65536 limbs)", "value": round(gl_b, 3),
+            "unit": "Glimbs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(batched_ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64 (GF(p), p=2^64-2^32+1)",
+            "data": "synthetic: seeded uniform random u32 limbs; lengths floor(2^(6+10u)), u uniform",
+            "config": {"workload": "4096 independent products, na and nb log-uniform in [64, 65536] limbs",
+                       "jobs": len(sizes), "total_input_limbs": total_limbs,
+                       "batch": "one CUDA-graph launch per step, size-bucketed, autotuned plans",
+                       "plan_and_autotune_s": round(plan_s, 2)},
+            "one_at_a_time": {"value": round(gl_s, 3), "unit": "Glimbs/s", "ms": round(single_ms, 3),
+                              "path": "one b2m_mul_device call per product on the same stream"},
+            "speedup_vs_one_at_a_time": round(single_ms / batched_ms, 2),
+            "bit_exact_vs_one_at_a_time": same,
+            "clocks": clocks}), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["single", "batch"], default="single",
+                    help="single: the 2^24-limb product (headline); batch: 4096 log-uniform pairs")
+    ap.add_argument("--batch-jobs", type=int, default=4096)
     ap.add_argument("--na", type=int, default=NA)
     ap.add_argument("--nb", type=int, default=NB)
     ap.add_argument("--e2e-steps", type=int, default=20)
@@ -380,6 +497,8 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch":
+        run_batch(args)
     else:
         run_ours(args)
 
