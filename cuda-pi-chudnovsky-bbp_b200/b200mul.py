@@ -246,3 +246,103 @@ def mul_batch(jobs, stream: int = 0) -> None:
     """One-shot batch (no graph), synchronous on `stream`."""
     arr = _jobs(jobs)
     check(lib.b2m_mul_batch(arr, len(jobs), stream or None), "b2m_mul_batch")
+
+
+# ---- Chudnovsky binary splitting ---------------------------------------------------
+_sig("b2m_chudnovsky_bs", ctypes.c_int, [_u64, _u64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)])
+_sig("b2m_pqt_info", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(_u64), ctypes.POINTER(ctypes.c_int32),
+                                    ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(_u64)])
+_sig("b2m_pqt_device", ctypes.c_void_p, [ctypes.c_void_p, ctypes.c_int])
+_sig("b2m_pqt_copy", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _u32p, _u64])
+_sig("b2m_pqt_free", ctypes.c_int, [ctypes.c_void_p])
+
+
+class PQT:
+    """Device-resident (P, Q, T) of a Chudnovsky term range (b2m_pqt)."""
+
+    def __init__(self, handle):
+        self.handle = handle
+        ln = (_u64 * 3)()
+        sg = ctypes.c_int32()
+        lv = ctypes.c_uint32()
+        pr = _u64()
+        check(lib.b2m_pqt_info(handle, ln, ctypes.byref(sg), ctypes.byref(lv), ctypes.byref(pr)), "b2m_pqt_info")
+        self.lengths = [int(x) for x in ln]
+        self.t_sign = int(sg.value)
+        self.levels = int(lv.value)
+        self.products = int(pr.value)
+
+    def limbs(self, which: int) -> np.ndarray:
+        out = np.zeros(max(1, self.lengths[which]), np.uint32)
+        check(lib.b2m_pqt_copy(self.handle, which, out.ctypes.data_as(_u32p), out.size), "b2m_pqt_copy")
+        return out[: self.lengths[which]]
+
+    def signed(self):
+        """[(sign, magnitude)] for P, Q, T, as the reference's BigInt holds them."""
+        return [(1 if self.lengths[0] else 0, self.limbs(0)), (1 if self.lengths[1] else 0, self.limbs(1)),
+                (self.t_sign, self.limbs(2))]
+
+    def free(self) -> None:
+        if self.handle:
+            check(lib.b2m_pqt_free(self.handle), "b2m_pqt_free")
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def chudnovsky_bs(a: int, b: int, stream: int = 0) -> PQT:
+    """Reference: chudnovsky_bs(a, b) (src/chudnovsky.cpp:64-102), on the device."""
+    h = ctypes.c_void_p()
+    check(lib.b2m_chudnovsky_bs(a, b, stream or None, ctypes.byref(h)), "b2m_chudnovsky_bs")
+    return PQT(h)
+
+
+DIGITS_PER_TERM = 14.181647462725477  # src/chudnovsky.cpp:46
+
+
+def chudnovsky_terms_for_digits(digits: int) -> int:
+    """Reference: chudnovsky_terms_for_digits (src/chudnovsky.cpp:54-59)."""
+    n = int(float(digits) / DIGITS_PER_TERM) + 2
+    return max(n, 2)
+
+
+def _to_int(limbs: np.ndarray) -> int:
+    return int.from_bytes(np.ascontiguousarray(limbs, dtype="<u4").tobytes(), "little")
+
+
+def compute_pi(digits: int, timings: dict | None = None) -> str:
+    """Reference: compute_pi_chudnovsky (src/chudnovsky.cpp:107-164).
+
+    Same guard digits, term count, isqrt of 10005 * 10^(2 prec), floor
+    division and formatting; the binary-splitting tree runs on the device
+    (b2m_chudnovsky_bs) and the final assembly uses exact host integers."""
+    import math
+    import sys
+    import time
+
+    if hasattr(sys, "set_int_max_str_digits"):
+        sys.set_int_max_str_digits(0)
+    prec = digits + 16
+    n = chudnovsky_terms_for_digits(prec)
+    t0 = time.perf_counter()
+    r = chudnovsky_bs(0, n)
+    q = _to_int(r.limbs(1))
+    t = _to_int(r.limbs(2))
+    sign = r.t_sign
+    r.free()
+    t1 = time.perf_counter()
+    one = 10 ** prec
+    sqrt_c = math.isqrt(10005 * one * one)
+    numerator = q * 426880 * sqrt_c
+    pi_scaled = numerator // (t if sign > 0 else -t)
+    s = str(pi_scaled)
+    t2 = time.perf_counter()
+    if timings is not None:
+        timings.update({"terms": n, "tree_s": t1 - t0, "assembly_s": t2 - t1})
+    if digits == 0:
+        return "3"
+    return s[0] + "." + s[1:1 + digits]

@@ -161,6 +161,31 @@ b2m_status b2m_batch_destroy(b2m_batch* batch);
 /* create + launch + destroy without a graph: for one-shot batches. */
 b2m_status b2m_mul_batch(const b2m_job* jobs, uint64_t njobs, b2m_stream stream);
 
+/* ---- Chudnovsky binary splitting ------------------------------------------------
+ * Replaces chudnovsky_bs (src/chudnovsky.cpp:64-102) for the caller's
+ * product tree: (P, Q, T) of the term range [a, b), built level by level on
+ * the device with every value resident in HBM and every level's products
+ * batched (see b2m_chudnovsky.cu). The root equals the reference's
+ * (P and Q are products, T/Q the exact partial sum, so the tree shape does not
+ * matter). Term indices must stay below 2,000,000 (about 28 million digits). */
+
+typedef struct b2m_pqt b2m_pqt;  /* device-resident (P, Q, T) */
+
+b2m_status b2m_chudnovsky_bs(uint64_t a, uint64_t b, b2m_stream stream, b2m_pqt** result);
+
+/* Lengths (limbs) of P, Q, T, the sign of T (P, Q > 0), the number of tree
+ * levels and of products computed. Any pointer may be NULL. */
+b2m_status b2m_pqt_info(const b2m_pqt* r, uint64_t len[3], int32_t* t_sign, uint32_t* levels,
+                        uint64_t* products);
+
+/* Device pointer of P (which = 0), Q (1) or T's magnitude (2). */
+const uint32_t* b2m_pqt_device(const b2m_pqt* r, int which);
+
+/* Copies P, Q or |T| to host memory (cap limbs available). */
+b2m_status b2m_pqt_copy(const b2m_pqt* r, int which, uint32_t* host, uint64_t cap);
+
+b2m_status b2m_pqt_free(b2m_pqt* r);
+
 /* ---- plan inspection and tracing -------------------------------------------- */
 
 /* Kernel kinds of a product's launch sequence. */

@@ -128,3 +128,5 @@ if __name__ == "__main__":
         make_chudnovsky([10000000])
     if "pi" in what:
         make_pi([1000, 3500, 10000, 100000])
+    if "pi1m" in what:
+        make_pi([1000, 3500, 10000, 100000, 1000000])
