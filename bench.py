@@ -477,14 +477,189 @@ def run_batch(args) -> None:
         dist.destroy_process_group()
 
 
+def run_chudnovsky(args) -> None:
+    """Chudnovsky binary splitting for `--digits` digits (default 10^7): the
+    whole (P, Q, T) tree on the device, root checked against the reference."""
+    import hashlib
+
+    import numpy as np
+    import torch
+
+    import b200mul
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    b200mul.init(local)
+    terms = b200mul.chudnovsky_terms_for_digits(args.digits + 16)
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    for _ in range(args.warmup):
+        b200mul.chudnovsky_bs(0, terms, sp).free()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    walls = []
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r = b200mul.chudnovsky_bs(0, terms, sp)
+        walls.append(time.perf_counter() - t0)
+        if _ < args.steps - 1:
+            r.free()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    dev_ms = e0.elapsed_time(e1) / args.steps
+    # end to end: tree + copy of the root's P, Q, T to host memory
+    t0 = time.perf_counter()
+    hq = [r.limbs(w) for w in range(3)]
+    copy_s = time.perf_counter() - t0
+    def sha(x):
+        return hashlib.sha256(np.ascontiguousarray(x, dtype="<u4").tobytes()).hexdigest()
+    fixture = os.path.join(ROOT, "tests", "golden", "chudnovsky.json")
+    exact, ref_s = None, None
+    if os.path.exists(fixture):
+        trees = {t["terms"]: t for t in json.load(open(fixture))["trees"]}
+        if terms in trees:
+            tr = trees[terms]
+            exact = all(sha(hq[w]) == tr[nm]["sha256"] for w, nm in enumerate("PQT")) and r.t_sign == tr["T"]["sign"]
+            ref_s = tr["ref_s"]
+    levels, products, lengths = r.levels, r.products, r.lengths
+    r.free()
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        oracle_mod, kind, _ = _ref_or_port()
+        sample_digits = 1000000
+        st = b200mul.chudnovsky_terms_for_digits(sample_digits + 16)
+        t0 = time.perf_counter()
+        if kind == "reference":
+            oracle_mod.bs_ref(0, st, "ntt-cpu")
+        else:
+            oracle_mod.bs_port(0, st)
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(dt * 1e3, 1), "unit": "ms", "cores": 1, "kind": kind,
+               "sample": f"the reference's chudnovsky_bs(0, {st}) (1,000,000 digits, NttCpu backend, 1 thread) "
+                         f"timed on this host: {dt:.2f} s; its 10,000,000-digit tree took {ref_s} s on the "
+                         "build container's host (tests/golden/chudnovsky.json)"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": f"ms per Chudnovsky binary-splitting tree ({args.digits} digits)",
+            "value": round(statistics.median(walls) * 1e3, 2), "unit": "ms", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(dev_ms, 2), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs / u64 GF(p)",
+            "data": "deterministic: the Chudnovsky series terms",
+            "config": {"workload": f"chudnovsky_bs(0, {terms}) for {args.digits} digits, level-wise on device",
+                       "terms": terms, "levels": levels, "products": products,
+                       "root_limbs": {"P": lengths[0], "Q": lengths[1], "T": lengths[2]}},
+            "bit_exact_vs_reference_root": exact,
+            "reference_cpu_tree_s": ref_s,
+            "e2e": {"value": round((statistics.median(walls) + copy_s) * 1e3, 2), "unit": "ms",
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 4 * sum(lengths),
+                    "path": "b2m_chudnovsky_bs + copy of the root to host"},
+            "cpu_baseline": cpu, "clocks": clocks}), flush=True)
+
+
+def run_serve(args) -> None:
+    """Serving: Poisson arrivals at --rate req/s for --duration s, operand
+    lengths log-uniform in [2^10, 2^24] limbs, seeded operands generated on
+    the device, continuous batching under an HBM budget; p50/p99 latency and
+    throughput, every product residue-checked on the device."""
+    import numpy as np
+    import torch
+
+    import b200mul
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    b200mul.init(local)
+    rng = np.random.default_rng(2000 + rank)
+    n_req = int(args.rate * args.duration)
+    gaps = rng.exponential(1.0 / args.rate, n_req)
+    arrivals = np.cumsum(gaps)
+    lens = (2.0 ** rng.uniform(10, 24, (n_req, 2))).astype(np.int64)
+    srv = b200mul.Server(hbm_budget_bytes=args.serve_budget_gb << 30, streams=args.serve_streams,
+                         max_batch=args.serve_batch)
+    # warm-up: a few requests of every octave so pools and kernels are ready
+    warm = [srv.submit(1 << k, 1 << k, 99 + k, 199 + k) for k in range(10, 25, 2)]
+    for t in warm:
+        srv.wait(t, 120.0)
+        srv.release(t)
+    sampler = ClockSampler(local)
+    sampler.start()
+    outstanding = []
+    lat, done_t, bad, limbs_done = [], [], 0, 0
+    t0 = time.perf_counter()
+    i = 0
+
+    def reap(block: bool):
+        nonlocal bad, limbs_done
+        while outstanding:
+            t, na, nb = outstanding[0]
+            r = srv.poll(t) if not block else srv.wait(t, 300.0)
+            if r.state < b200mul.DONE:
+                return
+            outstanding.pop(0)
+            if r.state != b200mul.DONE or r.residues_ok != 1:
+                bad += 1
+            lat.append((r.t_done_ns - r.t_submit_ns) * 1e-6)
+            done_t.append(r.t_done_ns)
+            limbs_done += na + nb
+            srv.release(t)
+
+    while i < n_req:
+        now = time.perf_counter() - t0
+        while i < n_req and arrivals[i] <= now:
+            na, nb = int(lens[i, 0]), int(lens[i, 1])
+            outstanding.append((srv.submit(na, nb, 7 * i + 1, 7 * i + 2), na, nb))
+            i += 1
+        reap(False)
+        nxt = arrivals[i] if i < n_req else now
+        time.sleep(max(0.0, min(0.0005, nxt - (time.perf_counter() - t0))))
+    submit_end = time.perf_counter() - t0
+    reap(True)
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    st = srv.stats()
+    srv.stop()
+    lat = np.array(lat)
+    offered_limbs = int(lens.sum())
+    if rank == 0:
+        print(json.dumps({
+            "metric": "serve p50/p99 latency ms (Poisson arrivals, log-uniform 2^10..2^24 limbs)",
+            "value": round(float(np.percentile(lat, 50)), 2), "unit": "ms",
+            "p99_ms": round(float(np.percentile(lat, 99)), 2), "mean_ms": round(float(lat.mean()), 2),
+            "n_gpus": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u64 (GF(p), p=2^64-2^32+1)",
+            "data": "synthetic: seeded random limbs generated on the device per request",
+            "config": {"workload": f"{args.rate} req/s Poisson for {args.duration} s", "requests": n_req,
+                       "hbm_budget_gb": args.serve_budget_gb, "streams": args.serve_streams,
+                       "max_batch": args.serve_batch, "submit_window_s": round(submit_end, 2)},
+            "throughput": {"req_per_s": round(n_req / wall, 1), "glimbs_per_s": round(limbs_done / wall / 1e9, 3),
+                           "offered_glimbs_per_s": round(offered_limbs / args.duration / 1e9, 3),
+                           "wall_s": round(wall, 2)},
+            "all_products_residue_checked_ok": bad == 0, "failed_or_mismatched": bad,
+            "server": st, "clocks": clocks}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["single", "batch"], default="single",
-                    help="single: the 2^24-limb product (headline); batch: 4096 log-uniform pairs")
+    ap.add_argument("--workload", choices=["single", "batch", "chudnovsky", "serve"], default="single",
+                    help="single: the 2^24-limb product (headline); batch: 4096 log-uniform pairs; "
+                         "chudnovsky: the binary-splitting tree; serve: Poisson request stream")
+    ap.add_argument("--digits", type=int, default=10000000)
+    ap.add_argument("--rate", type=float, default=2000.0, help="serve: Poisson arrival rate (req/s)")
+    ap.add_argument("--duration", type=float, default=10.0, help="serve: seconds of arrivals")
+    ap.add_argument("--serve-budget-gb", type=int, default=120)
+    ap.add_argument("--serve-streams", type=int, default=4)
+    ap.add_argument("--serve-batch", type=int, default=64)
     ap.add_argument("--batch-jobs", type=int, default=4096)
     ap.add_argument("--na", type=int, default=NA)
     ap.add_argument("--nb", type=int, default=NB)
@@ -499,6 +674,10 @@ def main():
         run_reference(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "chudnovsky":
+        run_chudnovsky(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 

@@ -346,3 +346,85 @@ def compute_pi(digits: int, timings: dict | None = None) -> str:
     if digits == 0:
         return "3"
     return s[0] + "." + s[1:1 + digits]
+
+
+# ---- serving ------------------------------------------------------------------------
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", _u64), ("streams", ctypes.c_uint32), ("max_batch", ctypes.c_uint32),
+                ("max_pending", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("a", ctypes.c_void_p), ("na", _u64), ("b", ctypes.c_void_p), ("nb", _u64), ("seed_a", _u64),
+                ("seed_b", _u64), ("kind", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("out", ctypes.c_void_p), ("out_cap", _u64)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int32), ("status", ctypes.c_int), ("out", ctypes.c_void_p), ("out_len", _u64),
+                ("t_submit_ns", _u64), ("t_admit_ns", _u64), ("t_done_ns", _u64), ("residues_ok", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(n, _u64) for n in ("submitted", "completed", "failed", "dispatches", "inflight_dispatches",
+                                    "queued", "max_queue", "bytes_in_use", "peak_bytes")]
+
+
+_sig("b2m_server_start", ctypes.c_int, [ctypes.POINTER(ServerConfig), ctypes.POINTER(ctypes.c_void_p)])
+_sig("b2m_server_submit", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Request), ctypes.POINTER(_u64)])
+_sig("b2m_server_poll", ctypes.c_int, [ctypes.c_void_p, _u64, ctypes.POINTER(Result)])
+_sig("b2m_server_wait", ctypes.c_int, [ctypes.c_void_p, _u64, ctypes.c_double, ctypes.POINTER(Result)])
+_sig("b2m_server_release", ctypes.c_int, [ctypes.c_void_p, _u64])
+_sig("b2m_server_get_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerStats)])
+_sig("b2m_server_stop", ctypes.c_int, [ctypes.c_void_p])
+_sig("b2m_gen_operand", ctypes.c_int, [_u64, _u64, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p])
+
+QUEUED, RUNNING, DONE, FAILED = 0, 1, 2, 3
+
+
+def gen_operand_device(seed: int, n: int, kind: int, ptr: int, stream: int = 0) -> None:
+    """Device copy of gen_operand (b2m_gen_operand)."""
+    check(lib.b2m_gen_operand(seed, n, kind, ptr, stream or None), "b2m_gen_operand")
+
+
+class Server:
+    """Continuous-batching multiply server (b2m_server_*)."""
+
+    def __init__(self, hbm_budget_bytes: int = 0, streams: int = 0, max_batch: int = 0, max_pending: int = 0):
+        cfg = ServerConfig(hbm_budget_bytes, streams, max_batch, max_pending, 0)
+        self.handle = ctypes.c_void_p()
+        check(lib.b2m_server_start(ctypes.byref(cfg), ctypes.byref(self.handle)), "b2m_server_start")
+
+    def submit(self, na: int, nb: int, seed_a: int = 0, seed_b: int = 0, kind: int = 0, a: int = 0, b: int = 0,
+               out: int = 0, out_cap: int = 0) -> int:
+        req = Request(a or None, na, b or None, nb, seed_a, seed_b, kind, 0, out or None, out_cap)
+        t = _u64()
+        check(lib.b2m_server_submit(self.handle, ctypes.byref(req), ctypes.byref(t)), "b2m_server_submit")
+        return t.value
+
+    def poll(self, ticket: int) -> Result:
+        r = Result()
+        check(lib.b2m_server_poll(self.handle, ticket, ctypes.byref(r)), "b2m_server_poll")
+        return r
+
+    def wait(self, ticket: int, timeout_s: float = 60.0) -> Result:
+        r = Result()
+        st = lib.b2m_server_wait(self.handle, ticket, timeout_s, ctypes.byref(r))
+        if st not in (OK, DEVICE_TIMEOUT):
+            check(st, "b2m_server_wait")
+        return r
+
+    def release(self, ticket: int) -> None:
+        check(lib.b2m_server_release(self.handle, ticket), "b2m_server_release")
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        check(lib.b2m_server_get_stats(self.handle, ctypes.byref(s)), "b2m_server_get_stats")
+        return {n: int(getattr(s, n)) for n, _ in ServerStats._fields_}
+
+    def stop(self) -> None:
+        if self.handle:
+            check(lib.b2m_server_stop(self.handle), "b2m_server_stop")
+            self.handle = ctypes.c_void_p()
+

@@ -25,16 +25,6 @@
 
 namespace b2m {
 
-// Zero the carry scratch of every multi-pass job and every job's out_len
-// (multi-pass products accumulate it with atomicMax; empty jobs report 0).
-__global__ void k_batch_prep(const ProdJob* __restrict__ jobs, unsigned njobs, unsigned long long* scratch,
-                             u64 nwords) {
-    const u64 stride = (u64)gridDim.x * blockDim.x;
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < nwords; i += stride) scratch[i] = 0;
-    for (u64 j = (u64)blockIdx.x * blockDim.x + threadIdx.x; j < njobs; j += stride)
-        if (jobs[j].out_len) *jobs[j].out_len = 0;
-}
-
 struct Bucket {
     int logn = 0;
     Plan plan;
@@ -66,9 +56,8 @@ namespace b2m {
 static cudaError_t enqueue_batch(b2m_batch* bt, cudaStream_t s) {
     Context* c = bt->ctx;
     cudaError_t e;
-    const unsigned prep_blocks = (unsigned)std::min<uint64_t>(1024, (bt->scratch_words + bt->njobs_all + 255) / 256 + 1);
-    k_batch_prep<<<prep_blocks, 256, 0, s>>>(bt->djobs, bt->njobs_all, bt->scratch, bt->scratch_words);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = launch_batch_prep(s, bt->djobs, bt->njobs_all, bt->scratch, bt->scratch_words)) != cudaSuccess)
+        return e;
     if ((e = cudaEventRecord(bt->ev[0], s)) != cudaSuccess) return e;
     const size_t ns = bt->side.size();
     for (size_t i = 0; i < ns; ++i)
@@ -116,12 +105,11 @@ static cudaError_t autotune_bucket(b2m_batch* bt, Bucket& b, cudaStream_t s) {
     cudaEventCreate(&t1);
     float best = 1e30f;
     Plan best_p = b.plan;
-    const unsigned prep_blocks = 1024;
     cudaError_t e = cudaSuccess;
     for (const Plan& p : cands) {
         float ms_sum = 0;
         for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
-            k_batch_prep<<<prep_blocks, 256, 0, s>>>(bt->djobs, bt->njobs_all, bt->scratch, bt->scratch_words);
+            launch_batch_prep(s, bt->djobs, bt->njobs_all, bt->scratch, bt->scratch_words);
             cudaEventRecord(t0, s);
             e = launch_bucket(p, bt->djobs + b.first, b.njobs, c->tw, c->d_err, s);
             cudaEventRecord(t1, s);

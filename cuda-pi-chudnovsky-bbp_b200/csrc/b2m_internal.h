@@ -90,6 +90,12 @@ struct Tracer {
 cudaError_t launch_bucket(const Plan& p, const ProdJob* jobs, unsigned njobs, const RootTables& tw, u32* err,
                           cudaStream_t s);
 
+// Zero `nwords` u64 of carry scratch and every job's out_len.
+cudaError_t launch_batch_prep(cudaStream_t s, const ProdJob* jobs, unsigned njobs, unsigned long long* scratch,
+                              u64 nwords);
+// Seeded operand generator (same sequence as b2m_gen_operand).
+cudaError_t launch_gen_operand(cudaStream_t s, u64 seed, u64 n, u32 kind, u32* out);
+
 cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb, u32* out,
                            uint64_t* out_len, void* ws, const Plan& plan, const RootTables& tw,
                            u32* err, cudaStream_t stream, Tracer* tr = nullptr);

@@ -204,4 +204,48 @@ cudaError_t launch_bucket(const Plan& p, const ProdJob* jobs, unsigned njobs, co
     return launch_carry(nchunks, s, nullptr, nullptr, 0, nullptr, nullptr, nullptr, err, jobs, njobs);
 }
 
+// Zero a contiguous carry-scratch region and every job's out_len
+// (multi-pass products accumulate it with atomicMax; empty jobs report 0).
+__global__ void k_batch_prep(const ProdJob* __restrict__ jobs, unsigned njobs, unsigned long long* scratch,
+                             u64 nwords) {
+    const u64 stride = (u64)gridDim.x * blockDim.x;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < nwords; i += stride) scratch[i] = 0;
+    for (u64 j = (u64)blockIdx.x * blockDim.x + threadIdx.x; j < njobs; j += stride)
+        if (jobs[j].out_len) *jobs[j].out_len = 0;
+}
+
+cudaError_t launch_batch_prep(cudaStream_t s, const ProdJob* jobs, unsigned njobs, unsigned long long* scratch,
+                              u64 nwords) {
+    const uint64_t work = nwords > njobs ? nwords : njobs;
+    const unsigned blocks = (unsigned)(work / 256 + 1 < 1024 ? work / 256 + 1 : 1024);
+    k_batch_prep<<<blocks, 256, 0, s>>>(jobs, njobs, scratch, nwords);
+    return cudaGetLastError();
+}
+
+// Seeded operands: limb i = high half of splitmix64's output function at
+// seed + (i + 1) * 0x9E3779B97F4A7C15, top limb forced non-zero; kind 1 gives
+// all-0xFFFFFFFF limbs.
+__device__ __forceinline__ u32 gen_limb(u64 seed, u64 i) {
+    u64 z = seed + (i + 1) * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return (u32)(z >> 32);
+}
+
+__global__ void k_gen_operand(u64 seed, u64 n, u32 kind, u32* out) {
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        u32 v = kind == 1 ? 0xFFFFFFFFu : gen_limb(seed, i);
+        if (i == n - 1 && v == 0) v = 1;
+        out[i] = v;
+    }
+}
+
+cudaError_t launch_gen_operand(cudaStream_t s, u64 seed, u64 n, u32 kind, u32* out) {
+    if (n == 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+    k_gen_operand<<<blocks, 256, 0, s>>>(seed, n, kind, out);
+    return cudaGetLastError();
+}
+
 }  // namespace b2m

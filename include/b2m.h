@@ -186,6 +186,71 @@ b2m_status b2m_pqt_copy(const b2m_pqt* r, int which, uint32_t* host, uint64_t ca
 
 b2m_status b2m_pqt_free(b2m_pqt* r);
 
+/* ---- serving ---------------------------------------------------------------------
+ * No counterpart in the reference. A continuous-batching multiply server:
+ * requests of mixed sizes are submitted at any time, admitted in arrival
+ * order while the server's HBM budget allows (generated operands, owned
+ * outputs and each product's transform workspace count against it), grouped
+ * into a dispatch whenever one of the server's stream slots is free, and run
+ * as size buckets on that slot's stream, so dispatches overlap on the device.
+ * Every product is checked on the device modulo 2^32 - 1 and 2^32 + 1 before
+ * it is reported done. */
+
+typedef struct b2m_server b2m_server;
+
+typedef struct b2m_server_config {
+    uint64_t hbm_budget_bytes;  /* device memory the server may hold (0 = half the library budget) */
+    uint32_t streams;           /* concurrent dispatches (0 = 4) */
+    uint32_t max_batch;         /* requests per dispatch (0 = 256) */
+    uint32_t max_pending;       /* queued requests before B2M_ERR_QUEUE_FULL (0 = 2^20) */
+    uint32_t reserved;
+} b2m_server_config;
+
+typedef struct b2m_request {
+    const uint32_t* a;          /* device operand, or NULL: generated from seed_a */
+    uint64_t na;
+    const uint32_t* b;          /* device operand, or NULL: generated from seed_b */
+    uint64_t nb;
+    uint64_t seed_a, seed_b;    /* generator of b2m_gen_operand */
+    uint32_t kind;              /* generated operands: 0 random limbs, 1 all 0xFFFFFFFF */
+    uint32_t reserved;
+    uint32_t* out;              /* device output (out_cap >= na + nb), or NULL: the server allocates it */
+    uint64_t out_cap;
+} b2m_request;
+
+typedef struct b2m_result {
+    int32_t state;              /* 0 queued, 1 on the GPU, 2 done, 3 failed */
+    b2m_status status;
+    uint32_t* out;              /* device pointer of the product (valid until b2m_server_release) */
+    uint64_t out_len;           /* trimmed length */
+    uint64_t t_submit_ns, t_admit_ns, t_done_ns;  /* steady-clock nanoseconds */
+    int32_t residues_ok;        /* product matched mod 2^32 - 1 and 2^32 + 1 */
+    int32_t reserved;
+} b2m_result;
+
+typedef struct b2m_server_stats {
+    uint64_t submitted, completed, failed, dispatches;
+    uint64_t inflight_dispatches, queued, max_queue;
+    uint64_t bytes_in_use, peak_bytes;
+} b2m_server_stats;
+
+b2m_status b2m_server_start(const b2m_server_config* cfg, b2m_server** server);
+b2m_status b2m_server_submit(b2m_server* server, const b2m_request* req, uint64_t* ticket);
+b2m_status b2m_server_poll(b2m_server* server, uint64_t ticket, b2m_result* result);
+/* Blocks until the request is done or failed, or the timeout passes
+ * (B2M_ERR_DEVICE_TIMEOUT, result still filled). */
+b2m_status b2m_server_wait(b2m_server* server, uint64_t ticket, double timeout_s, b2m_result* result);
+/* Forgets a finished request and frees the buffers the server owned for it. */
+b2m_status b2m_server_release(b2m_server* server, uint64_t ticket);
+b2m_status b2m_server_get_stats(b2m_server* server, b2m_server_stats* stats);
+/* Completes every queued and running request, then stops the scheduler. */
+b2m_status b2m_server_stop(b2m_server* server);
+
+/* Seeded operand on the device: limb i = high 32 bits of splitmix64's output
+ * function at seed + (i + 1) * 0x9E3779B97F4A7C15, top limb forced non-zero
+ * (kind 0), or all 0xFFFFFFFF limbs (kind 1). No reference counterpart. */
+b2m_status b2m_gen_operand(uint64_t seed, uint64_t n, uint32_t kind, uint32_t* d_out, b2m_stream stream);
+
 /* ---- plan inspection and tracing -------------------------------------------- */
 
 /* Kernel kinds of a product's launch sequence. */
