@@ -101,11 +101,107 @@ GL_FN u64 gl_reduce128(u64 lo, u64 hi) {
     return gl_fold32(t0, hl);
 }
 
-GL_FN u64 gl_mul(u64 a, u64 b) { return gl_reduce128(a * b, gl_mulhi(a, b)); }
+#if defined(__CUDA_ARCH__)
+// ---------------------------------------------------------------------------
+// Device folds on 32-bit words. A value V = H*2^32 + P - L with H < 2^32 and
+// -p < V < 2^64 is one borrow chain: on a borrow, V + p is the wrapped
+// difference minus EPS (the wrap added 2^64 = p + EPS).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ u64 gl_hpl(u32 H, u32 P, u32 Lc, u32 Ll) {
+    u32 d0, d1;
+    asm("{\n\t.reg .u32 m;\n\t"
+        "sub.cc.u32 %0, %3, %5;\n\t"
+        "subc.cc.u32 %1, %2, %4;\n\t"
+        "subc.u32 m, 0, 0;\n\t"
+        "sub.cc.u32 %0, %0, m;\n\t"
+        "subc.u32 %1, %1, 0;\n\t}"
+        : "=r"(d0), "=r"(d1)
+        : "r"(H), "r"(P), "r"(Lc), "r"(Ll));
+    return ((u64)d1 << 32) | d0;
+}
+
+// End-around sum of two words: (a + b) mod 2^32 plus the carry, and the carry.
+// For a + b <= 2^33 - 2 the result fits a word, and
+// (a + b) * 2^32 == result * 2^32 - carry (mod p) since 2^64 == 2^32 - 1.
+__device__ __forceinline__ u32 gl_ea_add(u32 a, u32 b, u32& c) {
+    u32 t;
+    asm("add.cc.u32 %0, %2, %3;\n\taddc.u32 %1, 0, 0;" : "=r"(t), "=r"(c) : "r"(a), "r"(b));
+    return t + c;
+}
+
+// a + b + c as a 33-bit value hi:lo.
+__device__ __forceinline__ void gl_add3(u32 a, u32 b, u32 c, u32& hi, u32& lo) {
+    asm("add.cc.u32 %0, %2, %3;\n\taddc.u32 %1, 0, 0;" : "=r"(lo), "=r"(hi) : "r"(a), "r"(b));
+    asm("add.cc.u32 %0, %0, %2;\n\taddc.u32 %1, %1, 0;" : "+r"(lo), "+r"(hi) : "r"(c));
+}
+
+__device__ __forceinline__ u64 gl_canon(u64 r) { return r >= GL_P ? r - GL_P : r; }
+#endif
+
+// a * b. Device: the 128-bit product r3:r2:r1:r0 from 32-bit multiply-adds,
+// then V == (r1 + r2)*2^32 + r0 - r2 - r3 folded with one end-around carry
+// and one borrow chain (range -2^33 < V < 2^64), and one range check.
+GL_FN u64 gl_mul(u64 a, u64 b) {
+#if defined(__CUDA_ARCH__)
+    const u32 a0 = (u32)a, a1 = (u32)(a >> 32), b0 = (u32)b, b1 = (u32)(b >> 32);
+    u32 r0, r1, r2, r3;
+    asm("mul.lo.u32 %0, %4, %6;\n\t"
+        "mul.hi.u32 %1, %4, %6;\n\t"
+        "mad.lo.cc.u32 %1, %4, %7, %1;\n\t"
+        "madc.hi.u32 %2, %4, %7, 0;\n\t"
+        "mad.lo.cc.u32 %1, %5, %6, %1;\n\t"
+        "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+        "addc.u32 %3, 0, 0;\n\t"
+        "mad.lo.cc.u32 %2, %5, %7, %2;\n\t"
+        "madc.hi.u32 %3, %5, %7, %3;"
+        : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+        : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+    u32 hc, lc, ll;
+    const u32 h = gl_ea_add(r1, r2, hc);
+    gl_add3(r2, r3, hc, lc, ll);
+    return gl_canon(gl_hpl(h, r0, lc, ll));
+#else
+    return gl_reduce128(a * b, gl_mulhi(a, b));
+#endif
+}
 
 // x * 2^s for canonical x and 0 <= s < 192. Written so that, with s known at
-// compile time (all register butterflies), every branch folds away.
+// compile time (the register butterflies), every branch folds away; with s
+// warp-uniform at run time the branches are uniform.
+//
+// Device: s = 96n + 32w + t (n, w, t digits). x*2^t = W2:W1:W0 (W2 < 2^t) from
+// two 32-bit multiply-adds, then per word offset w:
+//   w = 0:  V == (W1 + W2)*2^32 + W0 - W2
+//   w = 1:  V == (W0 + W1)*2^32 - (W1 + W2)          (no range check needed)
+//   w = 2:  V == W0*2^32 - ((W2 + c)*2^32 + lo(W0 + W1)), c its carry
+// each an end-around carry plus one borrow chain (gl_hpl); 2^96 == -1 negates.
 GL_FN u64 gl_shl(u64 x, int s) {
+#if defined(__CUDA_ARCH__)
+    if (s == 0) return x;
+    const bool neg = s >= 96;
+    if (neg) s -= 96;
+    const int t = s & 31, w = s >> 5;
+    u64 u, v;
+    asm("mul.wide.u32 %0, %1, %2;" : "=l"(u) : "r"((u32)x), "r"(1u << t));
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(v) : "r"((u32)(x >> 32)), "r"(1u << t), "l"(u >> 32));
+    const u32 W0 = (u32)u, W1 = (u32)v, W2 = (u32)(v >> 32);
+    u64 r;
+    if (w == 0) {
+        u32 hc;
+        const u32 h = gl_ea_add(W1, W2, hc);
+        r = gl_canon(gl_hpl(h, W0, 0, W2 + hc));
+    } else if (w == 1) {
+        u32 hc, lc, ll;
+        const u32 h = gl_ea_add(W0, W1, hc);
+        gl_add3(W1, W2, hc, lc, ll);
+        r = gl_hpl(h, 0, lc, ll);
+    } else {
+        u32 c, ll;
+        asm("add.cc.u32 %0, %2, %3;\n\taddc.u32 %1, 0, 0;" : "=r"(ll), "=r"(c) : "r"(W0), "r"(W1));
+        r = gl_hpl(W0, 0, W2 + c, ll);
+    }
+    return neg ? gl_sub(0, r) : r;
+#else
     bool neg = false;
     if (s >= 96) { s -= 96; neg = true; }   // 2^96 == -1
     u64 r;
@@ -124,6 +220,7 @@ GL_FN u64 gl_shl(u64 x, int s) {
         r = gl_sub(gl_reduce128(0, zl), zh << 32);
     }
     return neg ? gl_neg(r) : r;
+#endif
 }
 
 GL_FN u64 gl_pow(u64 b, u64 e) {
