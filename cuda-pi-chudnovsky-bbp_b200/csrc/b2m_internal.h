@@ -136,6 +136,7 @@ cudaError_t launch_carry(unsigned nchunks, cudaStream_t s, const u64* coef, u32*
                          const ProdJob* jobs = nullptr, unsigned njobs = 1);
 cudaError_t configure_first();
 cudaError_t configure_mid();
+cudaError_t configure_inv();
 cudaError_t configure_last();
 cudaError_t configure_fused();
 cudaError_t configure_small();

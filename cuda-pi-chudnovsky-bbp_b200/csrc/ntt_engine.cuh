@@ -81,45 +81,63 @@ constexpr int brev_c(int v, int bits) {
 
 enum { MAP_COL = 0, MAP_ROW = 1 };
 
-// Tile geometry. MAP_COL: columns are the fastest-varying index of task
-// enumeration and of the [R][C] shared layout (used when a row segment of C
-// columns is contiguous in global memory, S >= C). MAP_ROW: rows fastest and
-// a [C][R] layout (S == 1: every column is a contiguous sub-problem).
-// Shared memory is padded by one row every 64 rows against bank conflicts.
-template <int LOGR, int MAP>
+// Tile geometry, all compile-time: R = 2^LOGR rows by C = 2^LOGC columns,
+// T = max(1, R*C/16) threads, so every radix-8 level is two 8-point tasks per
+// thread and every load or store loop is 16 elements per thread.
+// MAP_COL: columns are the fastest-varying index of task enumeration and of
+// the [R][C] shared layout (used when a row segment of C columns is contiguous
+// in global memory, S >= C). MAP_ROW: rows fastest and a [C][R] layout (S == 1:
+// every column is a contiguous sub-problem). Shared memory is padded by one row
+// every 64 rows against bank conflicts.
+template <int LOGR, int LOGC, int MAP>
 struct Tile {
+    static constexpr int LR = LOGR, LC = LOGC, MAPK = MAP;
     static constexpr int R = 1 << LOGR;
+    static constexpr int C = 1 << LOGC;
     static constexpr int RP = R + (R >> 6);
-    int logC;
+    static constexpr int LOGT = LOGR + LOGC >= 4 ? LOGR + LOGC - 4 : 0;
+    static constexpr int T = 1 << LOGT;
 
-    __device__ __forceinline__ int saddr(int row, int col) const {
-        const int pr = row + (row >> 6);
-        return MAP == MAP_COL ? (pr << logC) + col : col * RP + pr;
+    static constexpr int pad(int row) { return row + (row >> 6); }
+    __device__ __forceinline__ static int saddr(int row, int col) {
+        return MAP == MAP_COL ? (pad(row) << LOGC) + col : col * RP + pad(row);
     }
     // Address step between rows S apart inside one task. Every task's rows
     // are either S >= 64 apart with S a multiple of 64, or all inside one
     // 64-row block, so the padded address is linear: base + m * step.
     template <int S>
-    __device__ __forceinline__ int step() const {
-        constexpr int PS = S >= 64 ? S + S / 64 : S;
-        return MAP == MAP_COL ? (PS << logC) : PS;
+    static constexpr int step() {
+        return MAP == MAP_COL ? ((S >= 64 ? S + S / 64 : S) << LOGC) : (S >= 64 ? S + S / 64 : S);
     }
-    // Instance q of a step with JW positions per block -> (col, blk, j).
-    __device__ __forceinline__ void decode(int q, int logjw, int& col, int& blk, int& j) const {
+    // Instance q of a step with 2^LOGJW positions per block -> (col, blk, j).
+    template <int LOGJW>
+    __device__ __forceinline__ static void decode(int q, int& col, int& blk, int& j) {
         if (MAP == MAP_COL) {
-            col = q & ((1 << logC) - 1);
-            const int r = q >> logC;
-            j = r & ((1 << logjw) - 1);
-            blk = r >> logjw;
+            col = q & (C - 1);
+            const int r = q >> LOGC;
+            j = r & ((1 << LOGJW) - 1);
+            blk = r >> LOGJW;
         } else {
-            j = q & ((1 << logjw) - 1);
-            const int r = q >> logjw;
-            const int lognb = LOGR - 6 - logjw;  // only used by radix-64 groups
-            blk = r & ((1 << lognb) - 1);
-            col = r >> lognb;
+            constexpr int LOGNB = LOGR - 6 - LOGJW;  // only used by radix-64 groups
+            j = q & ((1 << LOGJW) - 1);
+            const int r = q >> LOGJW;
+            blk = r & ((1 << LOGNB) - 1);
+            col = r >> LOGNB;
         }
     }
 };
+
+// Runs f(q) for the task indices q of this thread: TASKS tasks over T threads
+// (both powers of two), a rolled loop with a compile-time trip count.
+template <int TASKS, int T, typename F>
+__device__ __forceinline__ void for_tasks(F&& f) {
+    if constexpr (TASKS >= T) {
+#pragma unroll 1
+        for (int k = 0; k < TASKS / T; ++k) f((int)threadIdx.x + k * T);
+    } else {
+        if ((int)threadIdx.x < TASKS) f((int)threadIdx.x);
+    }
+}
 
 // Number of radix-8 levels and the leading radix exponent of a length-2^LOGR DFT.
 template <int LOGR>
@@ -135,22 +153,21 @@ struct Steps {
 // j in [0, R/2^A); elements at rows j + m*(R/2^A). Forward: DFT then
 // w_R^(j*k); inverse: w_R^(-j*k) then inverse DFT.
 // ---------------------------------------------------------------------------
-template <int LOGR, int MAP, int A, bool INV>
-__device__ __forceinline__ void lead_step(u64* sm, const Tile<LOGR, MAP>& tl, const u64* __restrict__ dtw) {
-    constexpr int E = 1 << A, R = 1 << LOGR, LOGJ = LOGR - A, JW = R >> A;
-    const int tasks = JW << tl.logC;
-    for (int q = threadIdx.x; q < tasks; q += blockDim.x) {
+template <class TL, int A, bool INV>
+__device__ __forceinline__ void lead_step(u64* sm, const u64* __restrict__ dtw) {
+    constexpr int E = 1 << A, R = TL::R, LOGJ = TL::LR - A, JW = R >> A;
+    for_tasks<(JW << TL::LC), TL::T>([&](int q) {
         int col, j;
-        if (MAP == MAP_COL) {
-            col = q & ((1 << tl.logC) - 1);
-            j = q >> tl.logC;
+        if (TL::MAPK == MAP_COL) {
+            col = q & (TL::C - 1);
+            j = q >> TL::LC;
         } else {
             j = q & (JW - 1);
             col = q >> LOGJ;
         }
         u64 x[E];
-        u64* ptr = sm + tl.saddr(j, col);
-        const int st = tl.template step<JW>();
+        u64* ptr = sm + TL::saddr(j, col);
+        constexpr int st = TL::template step<JW>();
 #pragma unroll
         for (int m = 0; m < E; ++m) x[m] = ptr[m * st];
         if (!INV) {
@@ -165,7 +182,7 @@ __device__ __forceinline__ void lead_step(u64* sm, const Tile<LOGR, MAP>& tl, co
         }
 #pragma unroll
         for (int m = 0; m < E; ++m) ptr[m * st] = x[m];
-    }
+    });
 }
 
 // ---------------------------------------------------------------------------
@@ -179,20 +196,19 @@ __device__ __forceinline__ void lead_step(u64* sm, const Tile<LOGR, MAP>& tl, co
 // Task order puts the level index (u1 or i1) outermost so it is uniform
 // across a warp whenever the tile has >= 32 instances.
 // ---------------------------------------------------------------------------
-template <int LOGR, int MAP, int LOGL, bool INV>
-__device__ __forceinline__ void group64(u64* sm, const Tile<LOGR, MAP>& tl, const u64* __restrict__ dtw) {
+template <class TL, int LOGL, bool INV>
+__device__ __forceinline__ void group64(u64* sm, const u64* __restrict__ dtw) {
     constexpr int L = 1 << LOGL, LOGJ = LOGL - 6, JW = 1 << LOGJ;
-    const int logni = LOGR - 6 + tl.logC;  // instances = C * R / 64
-    const int ni = 1 << logni;
-    const int tasks = ni << 3;
-    // ---- level 1 (forward) / level 1 inverse (second, for INV) ----
+    constexpr int LOGNI = TL::LR - 6 + TL::LC;  // instances = C * R / 64
+    constexpr int NI = 1 << LOGNI;
+    constexpr int TASKS = NI << 3;
     auto level1 = [&]() {
-        for (int q = threadIdx.x; q < tasks; q += blockDim.x) {
-            const int u1 = q >> logni;
+        for_tasks<TASKS, TL::T>([&](int q) {
+            const int u1 = q >> LOGNI;
             int col, blk, j;
-            tl.decode(q & (ni - 1), LOGJ, col, blk, j);
-            u64* ptr = sm + tl.saddr(blk * L + j + u1 * JW, col);
-            const int st = tl.template step<8 * JW>();
+            TL::template decode<LOGJ>(q & (NI - 1), col, blk, j);
+            u64* ptr = sm + TL::saddr(blk * L + j + u1 * JW, col);
+            constexpr int st = TL::template step<8 * JW>();
             u64 x[8];
 #pragma unroll
             for (int m = 0; m < 8; ++m) x[m] = ptr[m * st];
@@ -204,21 +220,21 @@ __device__ __forceinline__ void group64(u64* sm, const Tile<LOGR, MAP>& tl, cons
 #pragma unroll
                 for (int i = 1; i < 8; ++i) {
                     const int s = 3 * u1 * brev_c(i, 3);
-                    x[i] = s ? gl_shl(x[i], 192 - s) : x[i];
+                    x[i] = gl_shl(x[i], s ? 192 - s : 0);
                 }
                 dft_inv<8>(x);
             }
 #pragma unroll
             for (int m = 0; m < 8; ++m) ptr[m * st] = x[m];
-        }
+        });
     };
     auto level2 = [&]() {
-        for (int q = threadIdx.x; q < tasks; q += blockDim.x) {
-            const int i1 = q >> logni;
+        for_tasks<TASKS, TL::T>([&](int q) {
+            const int i1 = q >> LOGNI;
             int col, blk, j;
-            tl.decode(q & (ni - 1), LOGJ, col, blk, j);
-            u64* ptr = sm + tl.saddr(blk * L + j + i1 * 8 * JW, col);
-            const int st = tl.template step<JW>();
+            TL::template decode<LOGJ>(q & (NI - 1), col, blk, j);
+            u64* ptr = sm + TL::saddr(blk * L + j + i1 * 8 * JW, col);
+            constexpr int st = TL::template step<JW>();
             const int k1 = brev_c(i1, 3);
             u64 x[8];
 #pragma unroll
@@ -244,7 +260,7 @@ __device__ __forceinline__ void group64(u64* sm, const Tile<LOGR, MAP>& tl, cons
             }
 #pragma unroll
             for (int m = 0; m < 8; ++m) ptr[m * st] = x[m];
-        }
+        });
     };
     if (!INV) {
         level1();
@@ -258,21 +274,20 @@ __device__ __forceinline__ void group64(u64* sm, const Tile<LOGR, MAP>& tl, cons
 }
 
 // Trailing lone radix-8 level (L = 8, no twiddle): task (col, blk).
-template <int LOGR, int MAP, bool INV>
-__device__ __forceinline__ void lone8(u64* sm, const Tile<LOGR, MAP>& tl) {
-    constexpr int LOGNB = LOGR - 3;
-    const int tasks = 1 << (LOGNB + tl.logC);
-    for (int q = threadIdx.x; q < tasks; q += blockDim.x) {
+template <class TL, bool INV>
+__device__ __forceinline__ void lone8(u64* sm) {
+    constexpr int LOGNB = TL::LR - 3;
+    for_tasks<(1 << (LOGNB + TL::LC)), TL::T>([&](int q) {
         int col, blk;
-        if (MAP == MAP_COL) {
-            col = q & ((1 << tl.logC) - 1);
-            blk = q >> tl.logC;
+        if (TL::MAPK == MAP_COL) {
+            col = q & (TL::C - 1);
+            blk = q >> TL::LC;
         } else {
             blk = q & ((1 << LOGNB) - 1);
             col = q >> LOGNB;
         }
-        u64* ptr = sm + tl.saddr(blk * 8, col);
-        const int st = tl.template step<1>();
+        u64* ptr = sm + TL::saddr(blk * 8, col);
+        constexpr int st = TL::template step<1>();
         u64 x[8];
 #pragma unroll
         for (int m = 0; m < 8; ++m) x[m] = ptr[m * st];
@@ -280,54 +295,54 @@ __device__ __forceinline__ void lone8(u64* sm, const Tile<LOGR, MAP>& tl) {
         else dft_inv<8>(x);
 #pragma unroll
         for (int m = 0; m < 8; ++m) ptr[m * st] = x[m];
-    }
+    });
 }
 
 // Radix-64 groups from block size 2^LOGL down, G groups.
-template <int LOGR, int MAP, int LOGL, int G, bool INV>
-__device__ __forceinline__ void groups_fwd(u64* sm, const Tile<LOGR, MAP>& tl, const u64* dtw) {
+template <class TL, int LOGL, int G>
+__device__ __forceinline__ void groups_fwd(u64* sm, const u64* dtw) {
     if constexpr (G > 0) {
-        group64<LOGR, MAP, LOGL, false>(sm, tl, dtw);
+        group64<TL, LOGL, false>(sm, dtw);
         __syncthreads();
-        groups_fwd<LOGR, MAP, LOGL - 6, G - 1, false>(sm, tl, dtw);
+        groups_fwd<TL, LOGL - 6, G - 1>(sm, dtw);
     }
 }
-template <int LOGR, int MAP, int LOGL, int G>
-__device__ __forceinline__ void groups_inv(u64* sm, const Tile<LOGR, MAP>& tl, const u64* dtw) {
+template <class TL, int LOGL, int G>
+__device__ __forceinline__ void groups_inv(u64* sm, const u64* dtw) {
     // inverse order: smallest block first
     if constexpr (G > 0) {
-        groups_inv<LOGR, MAP, LOGL - 6, G - 1>(sm, tl, dtw);
-        group64<LOGR, MAP, LOGL, true>(sm, tl, dtw);
+        groups_inv<TL, LOGL - 6, G - 1>(sm, dtw);
+        group64<TL, LOGL, true>(sm, dtw);
         __syncthreads();
     }
 }
 
 // Whole column DFTs of the tile held in shared memory (callers synchronise
 // before; the functions end with the tile synchronised).
-template <int LOGR, int MAP>
-__device__ __forceinline__ void tile_fwd(u64* sm, const Tile<LOGR, MAP>& tl, const u64* dtw) {
-    using S = Steps<LOGR>;
+template <class TL>
+__device__ __forceinline__ void tile_fwd(u64* sm, const u64* dtw) {
+    using S = Steps<TL::LR>;
     if constexpr (S::A > 0) {
-        lead_step<LOGR, MAP, S::A, false>(sm, tl, dtw);
+        lead_step<TL, S::A, false>(sm, dtw);
         __syncthreads();
     }
-    groups_fwd<LOGR, MAP, LOGR - S::A, S::G, false>(sm, tl, dtw);
+    groups_fwd<TL, TL::LR - S::A, S::G>(sm, dtw);
     if constexpr (S::LONE) {
-        lone8<LOGR, MAP, false>(sm, tl);
+        lone8<TL, false>(sm);
         __syncthreads();
     }
 }
 
-template <int LOGR, int MAP>
-__device__ __forceinline__ void tile_inv(u64* sm, const Tile<LOGR, MAP>& tl, const u64* dtw) {
-    using S = Steps<LOGR>;
+template <class TL>
+__device__ __forceinline__ void tile_inv(u64* sm, const u64* dtw) {
+    using S = Steps<TL::LR>;
     if constexpr (S::LONE) {
-        lone8<LOGR, MAP, true>(sm, tl);
+        lone8<TL, true>(sm);
         __syncthreads();
     }
-    groups_inv<LOGR, MAP, LOGR - S::A, S::G>(sm, tl, dtw);
+    groups_inv<TL, TL::LR - S::A, S::G>(sm, dtw);
     if constexpr (S::A > 0) {
-        lead_step<LOGR, MAP, S::A, true>(sm, tl, dtw);
+        lead_step<TL, S::A, true>(sm, dtw);
         __syncthreads();
     }
 }

@@ -1,21 +1,34 @@
 // ntt_fam_fused.cu -- instantiations and launchers: fused last pass of operand B (forward, pointwise, inverse).
-// Kernel bodies are in ntt_kernels.cuh; one file per family keeps the
-// unrolled instantiations compiling in parallel. With a job table the grid's
-// second dimension (the first, for single-CTA products) runs over the jobs.
+// Written by gen_families.py; kernel bodies are in ntt_kernels.cuh. With a
+// job table the grid's second dimension (the first, for single-CTA
+// products) runs over the jobs.
 #include "ntt_kernels.cuh"
 
 namespace b2m {
 
 cudaError_t launch_fused_last(int logr, const PassGeo& g, cudaStream_t s, u64* bbuf, const u64* aspec, u64 ninv, const RootTables& tw, const ProdJob* jobs, unsigned njobs) {
-    switch (logr) {
-        case 7: k_fused_last<7><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, g.logc, ninv, tw, jobs); break;
-        case 8: k_fused_last<8><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, g.logc, ninv, tw, jobs); break;
-        case 9: k_fused_last<9><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, g.logc, ninv, tw, jobs); break;
-        case 10: k_fused_last<10><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, g.logc, ninv, tw, jobs); break;
-        case 11: k_fused_last<11><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, g.logc, ninv, tw, jobs); break;
-        case 12: k_fused_last<12><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, g.logc, ninv, tw, jobs); break;
-        case 13: k_fused_last<13><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, g.logc, ninv, tw, jobs); break;
-        case 14: k_fused_last<14><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, g.logc, ninv, tw, jobs); break;
+    switch (logr * 32 + g.logc) {
+        case 229: k_fused_last<7, 5><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 260: k_fused_last<8, 4><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 291: k_fused_last<9, 3><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 322: k_fused_last<10, 2><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 353: k_fused_last<11, 1><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 384: k_fused_last<12, 0><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 230: k_fused_last<7, 6><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 261: k_fused_last<8, 5><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 292: k_fused_last<9, 4><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 323: k_fused_last<10, 3><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 354: k_fused_last<11, 2><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 385: k_fused_last<12, 1><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 416: k_fused_last<13, 0><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 231: k_fused_last<7, 7><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 262: k_fused_last<8, 6><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 293: k_fused_last<9, 5><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 324: k_fused_last<10, 4><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 355: k_fused_last<11, 3><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 386: k_fused_last<12, 2><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 417: k_fused_last<13, 1><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 448: k_fused_last<14, 0><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
         default: return cudaErrorInvalidConfiguration;
     }
     return cudaGetLastError();
@@ -23,14 +36,27 @@ cudaError_t launch_fused_last(int logr, const PassGeo& g, cudaStream_t s, u64* b
 
 cudaError_t configure_fused() {
     cudaError_t e = cudaSuccess;
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<9>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<11>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<13>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<14>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<7, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<9, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<10, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<11, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<12, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<7, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<8, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<9, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<10, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<11, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<12, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<13, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<7, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<8, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<9, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<10, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<11, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<12, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<13, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<14, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     return e;
 }
 

@@ -1,7 +1,7 @@
 // ntt_fam_small.cu -- instantiations and launchers: single-CTA products, N <= 2^13.
-// Kernel bodies are in ntt_kernels.cuh; one file per family keeps the
-// unrolled instantiations compiling in parallel. With a job table the grid's
-// second dimension (the first, for single-CTA products) runs over the jobs.
+// Written by gen_families.py; kernel bodies are in ntt_kernels.cuh. With a
+// job table the grid's second dimension (the first, for single-CTA
+// products) runs over the jobs.
 #include "ntt_kernels.cuh"
 
 namespace b2m {

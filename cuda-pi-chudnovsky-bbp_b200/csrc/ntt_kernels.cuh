@@ -31,20 +31,9 @@ namespace b2m {
 
 constexpr int PASS_THREADS_MAX = 1024;
 
-// Global index of (row, column) in pass geometry (R = 2^LOGR, S = 2^logS):
-// column g = b*S + c belongs to sub-problem b, whose rows are S apart.
-template <int LOGR>
-__device__ __forceinline__ u64 pass_gidx(u64 g, int row, int logS) {
-    return ((g >> logS) << (LOGR + logS)) + ((u64)row << logS) + (g & ((1ull << logS) - 1));
-}
-
-// Exponent of the inter-pass twiddle w_M^(bitrev(row) * c), scaled to the
-// 2^32 root: x = (bitrev(row) * c) * 2^(32 - logM) mod 2^32.
-template <int LOGR>
-__device__ __forceinline__ u32 twiddle_exp(int row, u64 c, int logM) {
-    const u64 f = __brev((u32)row) >> (32 - LOGR);
-    return (u32)((f * c) << (32 - logM));
-}
+// Occupancy target of every pass kernel: 1024 resident threads per SM
+// (64 registers a thread), whatever the tile's thread count.
+#define B2M_PASS_BOUNDS(T) __launch_bounds__((T), (PASS_THREADS_MAX / (T)))
 
 __device__ __forceinline__ u64 digit_of(const u32* __restrict__ limbs, u64 ndig, u64 n) {
     if (n >= ndig) return 0;
@@ -52,15 +41,68 @@ __device__ __forceinline__ u64 digit_of(const u32* __restrict__ limbs, u64 ndig,
     return (n & 1) ? (u64)(w >> 16) : (u64)(w & 0xFFFFu);
 }
 
+// Column-mapped pass geometry (first, middle and non-last inverse passes).
+// The tile is rows [0, R) of columns [g0, g0 + C), C <= S, so all of it lies in
+// one sub-problem b = g0 >> logS. Thread t owns column col = t mod C and rows
+// row0 + k*DR (row0 = t / C, DR = R/16, k < 16): its global indices step by
+// DR*S, its shared addresses by a compile-time offset, and the bit-reversed
+// row is brev(row0) + brev(k*DR) (disjoint bits), so the inter-pass twiddle
+// exponent w_M^(brev(row) * c) is e0 + brev(k*DR) * (c << (32 - logM)).
+template <class TL>
+struct ColPass {
+    static constexpr int DR = TL::T >> TL::LC;
+    static constexpr int PER = (TL::R * TL::C) / TL::T;
+    static_assert(PER == 16 && DR >= 1, "16 elements per thread");
+    int col, row0, sa0;
+    u64 gi0, gstep;
+    u32 e0, ec;
+    __device__ __forceinline__ ColPass(int logS, int logM) {
+        col = (int)threadIdx.x & (TL::C - 1);
+        row0 = (int)threadIdx.x >> TL::LC;
+        sa0 = TL::saddr(row0, col);
+        const u64 g = ((u64)blockIdx.x << TL::LC) + col;
+        const u64 c = g & ((1ull << logS) - 1);
+        gi0 = ((g >> logS) << (TL::LR + logS)) + ((u64)row0 << logS) + c;
+        gstep = (u64)DR << logS;
+        const u32 sh = 32 - logM;
+        const u32 f0 = __brev((u32)row0) >> (32 - TL::LR);
+        ec = (u32)c << sh;
+        e0 = f0 * ec;
+    }
+    // shared-address offset and bit-reversed row part of element k
+    static constexpr int soff(int k) { return (k * DR + ((k * DR) >> 6)) << TL::LC; }
+    static constexpr u32 fk(int k) { return (u32)brev_c(k * DR, TL::LR); }
+};
+
+// Row-mapped (contiguous) tile of the last forward / first inverse pass:
+// element idx = t + k*T of the R*C block, row idx mod R, column idx / R.
+template <class TL>
+struct RowPass {
+    static_assert(TL::T >= 64, "row-mapped tiles have at least 64 threads");
+    static constexpr int PER = (TL::R * TL::C) / TL::T;
+    int sa0;
+    __device__ __forceinline__ RowPass() {
+        const int t = (int)threadIdx.x;
+        sa0 = TL::T >= TL::R ? TL::saddr(t & (TL::R - 1), t >> TL::LR) : TL::saddr(t, 0);
+    }
+    static constexpr int KR = TL::T >= TL::R ? 1 : TL::R / TL::T;  // loop steps per column
+    static constexpr int soff(int k) {
+        if (TL::T >= TL::R) return k * (TL::T >> TL::LR) * TL::RP;
+        const int kr = k % KR, kc = k / KR;
+        return kc * TL::RP + kr * TL::T + ((kr * TL::T) >> 6);
+    }
+};
+
 // ---------------------------------------------------------------------------
 // Pass 1 of a forward transform: u32 limbs read as 16-bit digits (digit n is
 // half n&1 of limb n>>1; digits at or past ndig are the zero padding).
 // ---------------------------------------------------------------------------
-template <int LOGR>
-__global__ void __launch_bounds__(PASS_THREADS_MAX) k_fwd_first(const u32* __restrict__ limbs, u64 ndig,
-                                                                u64* __restrict__ out, int logS, int logC,
-                                                                int logM, RootTables tw,
-                                                                const ProdJob* __restrict__ jobs, int operand) {
+template <int LOGR, int LOGC>
+__global__ void B2M_PASS_BOUNDS((Tile<LOGR, LOGC, MAP_COL>::T))
+k_fwd_first(const u32* __restrict__ limbs, u64 ndig, u64* __restrict__ out, int logS, int logM, RootTables tw,
+            const ProdJob* __restrict__ jobs, int operand) {
+    using TL = Tile<LOGR, LOGC, MAP_COL>;
+    using G = ColPass<TL>;
     extern __shared__ u64 sm[];
     if (jobs) {
         const ProdJob& J = jobs[blockIdx.y];
@@ -68,127 +110,115 @@ __global__ void __launch_bounds__(PASS_THREADS_MAX) k_fwd_first(const u32* __res
         ndig = 2 * (operand ? J.nb : J.na);
         out = operand ? J.bufB : J.bufA;
     }
-    const Tile<LOGR, MAP_COL> tl{logC};
-    const u64 g0 = (u64)blockIdx.x << logC;
-    const int cm = (1 << logC) - 1, total = (1 << LOGR) << logC;
-    const u64 smask = (1ull << logS) - 1;
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int col = idx & cm, row = idx >> logC;
-        sm[tl.saddr(row, col)] = digit_of(limbs, ndig, pass_gidx<LOGR>(g0 + col, row, logS));
-    }
+    const G gp(logS, logM);
+#pragma unroll
+    for (int k = 0; k < G::PER; ++k) sm[gp.sa0 + G::soff(k)] = digit_of(limbs, ndig, gp.gi0 + k * gp.gstep);
     __syncthreads();
-    tile_fwd<LOGR, MAP_COL>(sm, tl, tw.dtw);
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int col = idx & cm, row = idx >> logC;
-        const u64 g = g0 + col;
-        u64 x = sm[tl.saddr(row, col)];
-        const u32 e = twiddle_exp<LOGR>(row, g & smask, logM);
+    tile_fwd<TL>(sm, tw.dtw);
+#pragma unroll
+    for (int k = 0; k < G::PER; ++k) {
+        u64 x = sm[gp.sa0 + G::soff(k)];
+        const u32 e = gp.e0 + G::fk(k) * gp.ec;
         if (e) x = gl_mul(x, uroot(e, tw.u1, tw.u2));
-        out[pass_gidx<LOGR>(g, row, logS)] = x;
+        out[gp.gi0 + k * gp.gstep] = x;
     }
 }
 
 // A later, not-last forward pass, in place.
-template <int LOGR>
-__global__ void __launch_bounds__(PASS_THREADS_MAX) k_fwd_mid(u64* __restrict__ buf, int logS, int logC, int logM,
-                                                              RootTables tw, const ProdJob* __restrict__ jobs,
-                                                              int operand) {
+template <int LOGR, int LOGC>
+__global__ void B2M_PASS_BOUNDS((Tile<LOGR, LOGC, MAP_COL>::T))
+k_fwd_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const ProdJob* __restrict__ jobs, int operand) {
+    using TL = Tile<LOGR, LOGC, MAP_COL>;
+    using G = ColPass<TL>;
     extern __shared__ u64 sm[];
     if (jobs) buf = operand ? jobs[blockIdx.y].bufB : jobs[blockIdx.y].bufA;
-    const Tile<LOGR, MAP_COL> tl{logC};
-    const u64 g0 = (u64)blockIdx.x << logC;
-    const int cm = (1 << logC) - 1, total = (1 << LOGR) << logC;
-    const u64 smask = (1ull << logS) - 1;
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int col = idx & cm, row = idx >> logC;
-        sm[tl.saddr(row, col)] = buf[pass_gidx<LOGR>(g0 + col, row, logS)];
-    }
+    const G gp(logS, logM);
+#pragma unroll
+    for (int k = 0; k < G::PER; ++k) sm[gp.sa0 + G::soff(k)] = buf[gp.gi0 + k * gp.gstep];
     __syncthreads();
-    tile_fwd<LOGR, MAP_COL>(sm, tl, tw.dtw);
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int col = idx & cm, row = idx >> logC;
-        const u64 g = g0 + col;
-        u64 x = sm[tl.saddr(row, col)];
-        const u32 e = twiddle_exp<LOGR>(row, g & smask, logM);
+    tile_fwd<TL>(sm, tw.dtw);
+#pragma unroll
+    for (int k = 0; k < G::PER; ++k) {
+        u64 x = sm[gp.sa0 + G::soff(k)];
+        const u32 e = gp.e0 + G::fk(k) * gp.ec;
         if (e) x = gl_mul(x, uroot(e, tw.u1, tw.u2));
-        buf[pass_gidx<LOGR>(g, row, logS)] = x;
+        buf[gp.gi0 + k * gp.gstep] = x;
     }
 }
 
 // A not-last inverse pass, in place: inverse inter-pass twiddle on load, then
 // the inverse column DFTs. Pass 1 of the inverse leaves the convolution
 // coefficients (N^-1 already applied) in natural order.
-template <int LOGR>
-__global__ void __launch_bounds__(PASS_THREADS_MAX) k_inv_mid(u64* __restrict__ buf, int logS, int logC, int logM,
-                                                              RootTables tw, const ProdJob* __restrict__ jobs) {
+template <int LOGR, int LOGC>
+__global__ void B2M_PASS_BOUNDS((Tile<LOGR, LOGC, MAP_COL>::T))
+k_inv_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const ProdJob* __restrict__ jobs) {
+    using TL = Tile<LOGR, LOGC, MAP_COL>;
+    using G = ColPass<TL>;
     extern __shared__ u64 sm[];
     if (jobs) buf = jobs[blockIdx.y].bufB;
-    const Tile<LOGR, MAP_COL> tl{logC};
-    const u64 g0 = (u64)blockIdx.x << logC;
-    const int cm = (1 << logC) - 1, total = (1 << LOGR) << logC;
-    const u64 smask = (1ull << logS) - 1;
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int col = idx & cm, row = idx >> logC;
-        const u64 g = g0 + col;
-        u64 x = buf[pass_gidx<LOGR>(g, row, logS)];
-        const u32 e = twiddle_exp<LOGR>(row, g & smask, logM);
+    const G gp(logS, logM);
+#pragma unroll
+    for (int k = 0; k < G::PER; ++k) {
+        u64 x = buf[gp.gi0 + k * gp.gstep];
+        const u32 e = gp.e0 + G::fk(k) * gp.ec;
         if (e) x = gl_mul(x, uroot(0u - e, tw.u1, tw.u2));
-        sm[tl.saddr(row, col)] = x;
+        sm[gp.sa0 + G::soff(k)] = x;
     }
     __syncthreads();
-    tile_inv<LOGR, MAP_COL>(sm, tl, tw.dtw);
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int col = idx & cm, row = idx >> logC;
-        buf[pass_gidx<LOGR>(g0 + col, row, logS)] = sm[tl.saddr(row, col)];
-    }
+    tile_inv<TL>(sm, tw.dtw);
+#pragma unroll
+    for (int k = 0; k < G::PER; ++k) buf[gp.gi0 + k * gp.gstep] = sm[gp.sa0 + G::soff(k)];
 }
 
 // Last forward pass of operand A (S = 1: each column is a contiguous
 // sub-problem, so the CTA's tile is one contiguous range of R*C elements).
-template <int LOGR>
-__global__ void __launch_bounds__(PASS_THREADS_MAX) k_fwd_last(u64* __restrict__ buf, int logC, RootTables tw,
-                                                               const ProdJob* __restrict__ jobs) {
+template <int LOGR, int LOGC>
+__global__ void B2M_PASS_BOUNDS((Tile<LOGR, LOGC, MAP_ROW>::T))
+k_fwd_last(u64* __restrict__ buf, RootTables tw, const ProdJob* __restrict__ jobs) {
+    using TL = Tile<LOGR, LOGC, MAP_ROW>;
+    using G = RowPass<TL>;
     extern __shared__ u64 sm[];
     if (jobs) buf = jobs[blockIdx.y].bufA;
-    const Tile<LOGR, MAP_ROW> tl{logC};
-    u64* base = buf + ((u64)blockIdx.x << (LOGR + logC));
-    const int total = (1 << LOGR) << logC;
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x)
-        sm[tl.saddr(idx & ((1 << LOGR) - 1), idx >> LOGR)] = base[idx];
+    const G gp;
+    u64* base = buf + ((u64)blockIdx.x << (LOGR + LOGC)) + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < G::PER; ++k) sm[gp.sa0 + G::soff(k)] = base[k * TL::T];
     __syncthreads();
-    tile_fwd<LOGR, MAP_ROW>(sm, tl, tw.dtw);
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x)
-        base[idx] = sm[tl.saddr(idx & ((1 << LOGR) - 1), idx >> LOGR)];
+    tile_fwd<TL>(sm, tw.dtw);
+#pragma unroll
+    for (int k = 0; k < G::PER; ++k) base[k * TL::T] = sm[gp.sa0 + G::soff(k)];
 }
 
 // Last forward pass of operand B, pointwise product with A's spectrum (same
 // positions) and N^-1, then the first inverse pass -- one tile, one kernel.
-template <int LOGR>
-__global__ void __launch_bounds__(PASS_THREADS_MAX) k_fused_last(u64* __restrict__ bbuf, const u64* __restrict__ aspec,
-                                                                 int logC, u64 ninv, RootTables tw,
-                                                                 const ProdJob* __restrict__ jobs) {
+template <int LOGR, int LOGC>
+__global__ void B2M_PASS_BOUNDS((Tile<LOGR, LOGC, MAP_ROW>::T))
+k_fused_last(u64* __restrict__ bbuf, const u64* __restrict__ aspec, u64 ninv, RootTables tw,
+             const ProdJob* __restrict__ jobs) {
+    using TL = Tile<LOGR, LOGC, MAP_ROW>;
+    using G = RowPass<TL>;
     extern __shared__ u64 sm[];
     if (jobs) {
         bbuf = jobs[blockIdx.y].bufB;
         aspec = jobs[blockIdx.y].bufA;
     }
-    const Tile<LOGR, MAP_ROW> tl{logC};
-    const u64 off = (u64)blockIdx.x << (LOGR + logC);
+    const G gp;
+    const u64 off = ((u64)blockIdx.x << (LOGR + LOGC)) + threadIdx.x;
     u64* base = bbuf + off;
     const u64* abase = aspec + off;
-    const int total = (1 << LOGR) << logC;
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x)
-        sm[tl.saddr(idx & ((1 << LOGR) - 1), idx >> LOGR)] = base[idx];
+#pragma unroll
+    for (int k = 0; k < G::PER; ++k) sm[gp.sa0 + G::soff(k)] = base[k * TL::T];
     __syncthreads();
-    tile_fwd<LOGR, MAP_ROW>(sm, tl, tw.dtw);
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int a = tl.saddr(idx & ((1 << LOGR) - 1), idx >> LOGR);
-        sm[a] = gl_mul(gl_mul(sm[a], __ldg(abase + idx)), ninv);
+    tile_fwd<TL>(sm, tw.dtw);
+#pragma unroll
+    for (int k = 0; k < G::PER; ++k) {
+        u64& v = sm[gp.sa0 + G::soff(k)];
+        v = gl_mul(gl_mul(v, __ldg(abase + k * TL::T)), ninv);
     }
     __syncthreads();
-    tile_inv<LOGR, MAP_ROW>(sm, tl, tw.dtw);
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x)
-        base[idx] = sm[tl.saddr(idx & ((1 << LOGR) - 1), idx >> LOGR)];
+    tile_inv<TL>(sm, tw.dtw);
+#pragma unroll
+    for (int k = 0; k < G::PER; ++k) base[k * TL::T] = sm[gp.sa0 + G::soff(k)];
 }
 
 // ---------------------------------------------------------------------------
@@ -211,35 +241,34 @@ __global__ void __launch_bounds__(512) k_mul_small(const u32* __restrict__ a, u6
         nout = J.na + J.nb;
         out_len = J.out_len;
     }
-    using TL = Tile<LOGN, MAP_ROW>;
+    using TL = Tile<LOGN, 0, MAP_ROW>;
     constexpr int N = 1 << LOGN, RP = TL::RP, G = N < 16 ? N : 16;
     extern __shared__ u64 sm[];
     u64* smA = sm;
     u64* smB = sm + RP;
     CState* s_st = reinterpret_cast<CState*>(sm + 2 * RP);
     __shared__ unsigned long long s_top;
-    const TL tl{0};
     const u64 nda = 2 * na, ndb = 2 * nb;
     for (int i = threadIdx.x; i < N; i += blockDim.x) {
-        smA[tl.saddr(i, 0)] = digit_of(a, nda, i);
-        smB[tl.saddr(i, 0)] = digit_of(b, ndb, i);
+        smA[TL::saddr(i, 0)] = digit_of(a, nda, i);
+        smB[TL::saddr(i, 0)] = digit_of(b, ndb, i);
     }
     if (threadIdx.x == 0) s_top = 0;
     __syncthreads();
-    tile_fwd<LOGN, MAP_ROW>(smA, tl, tw.dtw);
-    tile_fwd<LOGN, MAP_ROW>(smB, tl, tw.dtw);
+    tile_fwd<TL>(smA, tw.dtw);
+    tile_fwd<TL>(smB, tw.dtw);
     for (int i = threadIdx.x; i < N; i += blockDim.x) {
-        const int s = tl.saddr(i, 0);
+        const int s = TL::saddr(i, 0);
         smB[s] = gl_mul(gl_mul(smB[s], smA[s]), ninv);
     }
     __syncthreads();
-    tile_inv<LOGN, MAP_ROW>(smB, tl, tw.dtw);
+    tile_inv<TL>(smB, tw.dtw);
 
     // Carry: thread t owns G consecutive coefficients.
     const int T = blockDim.x;
     u64 v[G];
 #pragma unroll
-    for (int i = 0; i < G; ++i) v[i] = smB[tl.saddr((int)threadIdx.x * G + i, 0)];
+    for (int i = 0; i < G; ++i) v[i] = smB[TL::saddr((int)threadIdx.x * G + i, 0)];
     u32 lm[G / 2];
     const CState st = group_carry<G>(v, lm);
     s_st[threadIdx.x] = st;

@@ -107,6 +107,7 @@ uint64_t workspace_bytes_for(int logn) {
 cudaError_t configure_kernels() {
     cudaError_t e = configure_first();
     if (e == cudaSuccess) e = configure_mid();
+    if (e == cudaSuccess) e = configure_inv();
     if (e == cudaSuccess) e = configure_last();
     if (e == cudaSuccess) e = configure_fused();
     if (e == cudaSuccess) e = configure_small();
