@@ -76,10 +76,14 @@ static void destroy_context(Context* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->hstream) cudaStreamSynchronize(c->hstream);
+    if (c->hcopy) cudaStreamSynchronize(c->hcopy);
     if (c->host_dev) cudaFree(c->host_dev);
     if (c->d_tables) cudaFree(c->d_tables);
     if (c->d_err) cudaFree(c->d_err);
     if (c->hstream) cudaStreamDestroy(c->hstream);
+    if (c->hcopy) cudaStreamDestroy(c->hcopy);
+    if (c->hev_a) cudaEventDestroy(c->hev_a);
+    if (c->hev_b) cudaEventDestroy(c->hev_b);
     delete c;
 }
 
@@ -155,7 +159,10 @@ b2m_status b2m_init(int device, uint64_t hbm_budget_bytes) {
     }
     if ((e = cudaMemcpy(c->d_tables, tables.data(), tbytes, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&c->d_err, 256)) != cudaSuccess || (e = cudaMemset(c->d_err, 0, 256)) != cudaSuccess ||
-        (e = cudaStreamCreateWithFlags(&c->hstream, cudaStreamNonBlocking)) != cudaSuccess) {
+        (e = cudaStreamCreateWithFlags(&c->hstream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&c->hcopy, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&c->hev_a, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&c->hev_b, cudaEventDisableTiming)) != cudaSuccess) {
         destroy_context(c);
         return cuda_status(e, "context setup");
     }
@@ -372,11 +379,19 @@ b2m_status b2m_mul_host(const uint32_t* a, uint64_t na, const uint32_t* b, uint6
     void* ws = base + ba + bb + bo + bl;
     cudaStream_t s = c->hstream;
     cudaError_t e;
+    // Operand B crosses the bus after A, on a second stream, while A's forward
+    // transform runs: the product waits for B only before B's transform.
     if ((e = cudaMemcpyAsync(da, a, 4 * na, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(db, b, 4 * nb, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        (e = cudaEventRecord(c->hev_a, s)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(c->hcopy, c->hev_a, 0)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(db, b, 4 * nb, cudaMemcpyHostToDevice, c->hcopy)) != cudaSuccess ||
+        (e = cudaEventRecord(c->hev_b, c->hcopy)) != cudaSuccess)
         return cuda_status(e, "cudaMemcpyAsync(H2D)");
-    if ((e = launch_product(da, na, db, nb, dout, dlen, ws, p, c->tw, c->d_err, s)) != cudaSuccess)
+    if ((e = launch_product(da, na, db, nb, dout, dlen, ws, p, c->tw, c->d_err, s, nullptr, c->hev_b)) !=
+        cudaSuccess) {
+        cudaStreamSynchronize(c->hcopy);
         return cuda_status(e, "kernel launch");
+    }
     uint64_t hlen = 0;
     if ((e = cudaMemcpyAsync(out, dout, 4 * (na + nb), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
         (e = cudaMemcpyAsync(&hlen, dlen, sizeof(uint64_t), cudaMemcpyDeviceToHost, s)) != cudaSuccess)

@@ -20,6 +20,8 @@ struct Context {
     RootTables tw{};
     u32* d_err = nullptr;                // sticky device error word (bounded waits)
     cudaStream_t hstream = nullptr;      // stream of the host-buffer entry point
+    cudaStream_t hcopy = nullptr;        // its second operand's H2D copy (overlaps operand A's transform)
+    cudaEvent_t hev_a = nullptr, hev_b = nullptr;  // operand A / operand B resident
     std::mutex host_mu;                  // serialises b2m_mul_host (shared buffers)
     void* host_dev = nullptr;            // device buffers of b2m_mul_host, grown on demand
     uint64_t host_dev_cap = 0;

@@ -98,7 +98,8 @@ cudaError_t launch_gen_operand(cudaStream_t s, u64 seed, u64 n, u32 kind, u32* o
 
 cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb, u32* out,
                            uint64_t* out_len, void* ws, const Plan& plan, const RootTables& tw,
-                           u32* err, cudaStream_t stream, Tracer* tr = nullptr);
+                           u32* err, cudaStream_t stream, Tracer* tr = nullptr,
+                           cudaEvent_t b_ready = nullptr);  // operand B waited for just before its transform
 // Kernels one product launches under plan p.
 int plan_launches(const Plan& p);
 

@@ -132,7 +132,7 @@ struct Tile {
 template <int TASKS, int T, typename F>
 __device__ __forceinline__ void for_tasks(F&& f) {
     if constexpr (TASKS >= T) {
-#pragma unroll 1
+#pragma unroll
         for (int k = 0; k < TASKS / T; ++k) f((int)threadIdx.x + k * T);
     } else {
         if ((int)threadIdx.x < TASKS) f((int)threadIdx.x);

@@ -133,7 +133,8 @@ static cudaError_t launch_forward(const u32* limbs, uint64_t nlimbs, u64* buf, c
 }
 
 cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb, u32* out, uint64_t* out_len,
-                           void* ws, const Plan& p, const RootTables& tw, u32* err, cudaStream_t s, Tracer* tr) {
+                           void* ws, const Plan& p, const RootTables& tw, u32* err, cudaStream_t s, Tracer* tr,
+                           cudaEvent_t b_ready) {
     const int logn = p.logn;
     const u64 ninv = gl_inv(1ull << logn);
     const u64 nout = na + nb;
@@ -144,6 +145,10 @@ cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb,
         g.grid = 1;
         g.block = (unsigned)T;
         g.smem = 2 * rp * sizeof(u64) + (size_t)T * 2 * sizeof(u64);
+        if (b_ready) {
+            cudaError_t e = cudaStreamWaitEvent(s, b_ready, 0);
+            if (e != cudaSuccess) return e;
+        }
         if (tr) tr->mark(s, B2M_K_SMALL, logn);
         cudaError_t e = launch_mul_small(logn, g, s, a, na, b, nb, out, nout,
                                          reinterpret_cast<unsigned long long*>(out_len), ninv, tw);
@@ -164,6 +169,7 @@ cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb,
     if (out_len && (e = cudaMemsetAsync(out_len, 0, sizeof(uint64_t), s)) != cudaSuccess) return e;
 
     if ((e = launch_forward(a, na, bufA, p, tw, false, nullptr, 0, s, tr)) != cudaSuccess) return e;
+    if (b_ready && (e = cudaStreamWaitEvent(s, b_ready, 0)) != cudaSuccess) return e;
     if ((e = launch_forward(b, nb, bufB, p, tw, true, bufA, ninv, s, tr)) != cudaSuccess) return e;
     for (int k = p.npass - 2; k >= 0; --k) {
         if (tr) tr->mark(s, B2M_K_INV_MID, p.logr[k]);
