@@ -120,11 +120,17 @@ __global__ void __launch_bounds__(CARRY_THREADS) k_carry(const u64* __restrict__
     const u64 lbase = cbase / 2;
     unsigned long long top = 0;
 #pragma unroll
-    for (int i = 0; i < CARRY_G / 2; ++i) {
-        if (lbase + i < nout) {
-            out[lbase + i] = lm[i];
-            if (lm[i]) top = lbase + i + 1;
-        }
+    for (int i = 0; i < CARRY_G / 2; ++i)
+        if (lm[i] && lbase + i < nout) top = lbase + i + 1;
+    if (lbase + CARRY_G / 2 <= nout && ((reinterpret_cast<uintptr_t>(out + lbase) & 15) == 0)) {
+        // whole group in range and 16-byte aligned: vector stores
+        uint4* dst = reinterpret_cast<uint4*>(out + lbase);
+#pragma unroll
+        for (int i = 0; i < CARRY_G / 8; ++i) dst[i] = make_uint4(lm[4 * i], lm[4 * i + 1], lm[4 * i + 2], lm[4 * i + 3]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < CARRY_G / 2; ++i)
+            if (lbase + i < nout) out[lbase + i] = lm[i];
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
