@@ -212,33 +212,21 @@ def run_ours(args) -> None:
     import torch
 
     import b200mul
+    import ranks
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    # Replicas: every rank multiplies its own pair (no data-path collective);
+    # the step time is the maximum over ranks.
+    rk = ranks.from_env("nccl", timeout_s=120)
+    rank, world, local = rk.rank, rk.world, rk.local
     torch.cuda.set_device(local)
     b200mul.init(local)
     na, nb = args.na, args.nb
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        ranks.barrier(rk)
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return ranks.max_over_ranks(rk, x)
 
     a_h = b200mul.gen_operand(SEED_A + 1000 * rank, na)
     b_h = b200mul.gen_operand(SEED_B + 1000 * rank, nb)
@@ -331,16 +319,22 @@ def run_ours(args) -> None:
 
     if rank == 0:
         value = step_ms / world
+        headline = na == NA and nb == NB
+        metric = METRIC if headline else f"ms per {na} x {nb}-limb multiply"
+        workload = ("2^24 x 2^24-limb product, uniform random limbs" if headline
+                    else f"{na} x {nb}-limb product, uniform random limbs")
+        wset = 4 * (na + nb) * 2 + 16 * n
         line = {
-            "metric": METRIC, "value": round(value, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "metric": metric, "value": round(value, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(step_ms, 4), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64 (GF(p), p=2^64-2^32+1)",
             "data": "synthetic: seeded uniform random u32 limbs (splitmix64), top limb non-zero",
-            "config": {"workload": "2^24 x 2^24-limb product, uniform random limbs", "na": na, "nb": nb,
+            "config": {"workload": workload, "na": na, "nb": nb,
                        "ntt_length": n, "plan": plan, "products_per_step": world,
                        "glimbs_per_s": round((na + nb) * world / (step_ms * 1e-3) / 1e9, 3),
-                       "l2": f"working set {(4 * (na + nb) * 2 + 16 * n) / 2**20:.0f} MiB per product "
-                             "> 126 MB L2: no flush needed"},
+                       "l2": f"working set {wset / 2**20:.0f} MiB per product "
+                             + ("> 126 MB L2: no flush needed" if wset > 126 * 2**20
+                                else "fits in the 126 MB L2: warm-cache figure")},
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
                          "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": round(dom_ms, 4),
@@ -359,8 +353,7 @@ def run_ours(args) -> None:
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    ranks.close(rk)
 
 
 def batch_sizes(n: int, seed: int):
@@ -380,22 +373,22 @@ def run_batch(args) -> None:
     import torch
 
     import b200mul
+    import ranks
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    rk = ranks.from_env("nccl", timeout_s=300)
+    rank, world, local = rk.rank, rk.world, rk.local
     torch.cuda.set_device(local)
     b200mul.init(local)
-    sizes = batch_sizes(args.batch_jobs, 4096 + rank)
+    if args.batch_split and world > 1:
+        # one batch of 4096 pairs, partitioned over the ranks by cost (LPT)
+        everything = batch_sizes(args.batch_jobs, 4096)
+        part = ranks.lpt_shard([ranks.product_cost(a, b) for a, b in everything], world)[rank]
+        sizes = [everything[i] for i in part]
+        job_limbs = sum(a + b for a, b in everything)
+    else:
+        # weak scaling: every rank its own 4096 pairs
+        sizes = batch_sizes(args.batch_jobs, 4096 + rank)
+        job_limbs = sum(a + b for a, b in sizes) * world
     total_limbs = sum(a + b for a, b in sizes)
     # Operands packed into one device tensor, outputs into two (batched, single).
     offs, tot = [], 0
@@ -451,21 +444,22 @@ def run_batch(args) -> None:
     bt.close()
     if not same:
         raise RuntimeError("batched and one-at-a-time products differ")
-    if dist is not None:
-        t = torch.tensor([batched_ms, single_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        batched_ms, single_ms = (float(x) for x in t.tolist())
+    if world > 1:
+        batched_ms, single_ms = ranks.max_over_ranks(rk, batched_ms, single_ms)
     if rank == 0:
-        gl_b = total_limbs * world / (batched_ms * 1e-3) / 1e9
-        gl_s = total_limbs * world / (single_ms * 1e-3) / 1e9
+        gl_b = job_limbs / (batched_ms * 1e-3) / 1e9
+        gl_s = job_limbs / (single_ms * 1e-3) / 1e9
         print(json.dumps({
             "metric": "batched Glimbs/s (4096 log-uniform pairs, 64..65536 limbs)", "value": round(gl_b, 3),
             "unit": "Glimbs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(batched_ms, 4), "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": round(batched_ms, 4), "higher_is_better": True,
+            "scaling": "strong" if (args.batch_split and world > 1) else "weak",
             "vs_baseline": None, "dtype": "u64 (GF(p), p=2^64-2^32+1)",
             "data": "synthetic: seeded uniform random u32 limbs; lengths floor(2^(6+10u)), u uniform",
             "config": {"workload": "4096 independent products, na and nb log-uniform in [64, 65536] limbs",
-                       "jobs": len(sizes), "total_input_limbs": total_limbs,
+                       "parallelism": ("one batch partitioned over the ranks by cost (LPT)"
+                                       if (args.batch_split and world > 1) else "one batch per rank"),
+                       "jobs_rank0": len(sizes), "input_limbs_all_ranks": job_limbs,
                        "batch": "one CUDA-graph launch per step, size-bucketed, autotuned plans",
                        "plan_and_autotune_s": round(plan_s, 2)},
             "one_at_a_time": {"value": round(gl_s, 3), "unit": "Glimbs/s", "ms": round(single_ms, 3),
@@ -473,8 +467,7 @@ def run_batch(args) -> None:
             "speedup_vs_one_at_a_time": round(single_ms / batched_ms, 2),
             "bit_exact_vs_one_at_a_time": same,
             "clocks": clocks}), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    ranks.close(rk)
 
 
 def run_chudnovsky(args) -> None:
@@ -486,33 +479,53 @@ def run_chudnovsky(args) -> None:
     import torch
 
     import b200mul
+    import ranks
 
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    rank = int(os.environ.get("RANK", "0"))
+    # One GPU: the whole tree. Several: one subtree per rank, roots merged
+    # pairwise into rank 0 (ranks.chudnovsky_bs_ranks) -- the same tree split
+    # over the GPUs, so the total work is fixed (strong scaling).
+    rk = ranks.from_env("nccl", timeout_s=300)
+    local, rank = rk.local, rk.rank
     torch.cuda.set_device(local)
     b200mul.init(local)
     terms = b200mul.chudnovsky_terms_for_digits(args.digits + 16)
     stream = torch.cuda.Stream()
     sp = stream.cuda_stream
+    backend = ranks.DeviceBackend(b200mul)
+
+    def tree():
+        if rk.world == 1:
+            return b200mul.chudnovsky_bs(0, terms, sp)
+        return ranks.chudnovsky_bs_ranks(rk, terms, backend)
+
     for _ in range(args.warmup):
-        b200mul.chudnovsky_bs(0, terms, sp).free()
+        t = tree()
+        if t is not None:
+            t.free()
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     walls = []
+    ranks.barrier(rk)
     torch.cuda.synchronize()
     e0.record(stream)
+    r = None
     for _ in range(args.steps):
+        ranks.barrier(rk)
         t0 = time.perf_counter()
-        r = b200mul.chudnovsky_bs(0, terms, sp)
-        walls.append(time.perf_counter() - t0)
-        if _ < args.steps - 1:
+        r = tree()
+        torch.cuda.synchronize()
+        walls.append(ranks.max_over_ranks(rk, time.perf_counter() - t0))
+        if _ < args.steps - 1 and r is not None:
             r.free()
     e1.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    dev_ms = e0.elapsed_time(e1) / args.steps
+    dev_ms = e0.elapsed_time(e1) / args.steps if rk.world == 1 else statistics.median(walls) * 1e3
+    if rank != 0:
+        ranks.close(rk)
+        return
     # end to end: tree + copy of the root's P, Q, T to host memory
     t0 = time.perf_counter()
     hq = [r.limbs(w) for w in range(3)]
@@ -530,7 +543,7 @@ def run_chudnovsky(args) -> None:
     levels, products, lengths = r.levels, r.products, r.lengths
     r.free()
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and rk.world == 1 and not args.no_cpu_baseline:
         oracle_mod, kind, _ = _ref_or_port()
         sample_digits = 1000000
         st = b200mul.chudnovsky_terms_for_digits(sample_digits + 16)
@@ -547,11 +560,14 @@ def run_chudnovsky(args) -> None:
     if rank == 0:
         print(json.dumps({
             "metric": f"ms per Chudnovsky binary-splitting tree ({args.digits} digits)",
-            "value": round(statistics.median(walls) * 1e3, 2), "unit": "ms", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(dev_ms, 2), "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs / u64 GF(p)",
+            "value": round(statistics.median(walls) * 1e3, 2), "unit": "ms", "n_gpus": rk.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dev_ms, 2),
+            "higher_is_better": False, "scaling": "strong" if rk.world > 1 else "weak",
+            "vs_baseline": None, "dtype": "u32 limbs / u64 GF(p)",
             "data": "deterministic: the Chudnovsky series terms",
             "config": {"workload": f"chudnovsky_bs(0, {terms}) for {args.digits} digits, level-wise on device",
+                       "parallelism": (f"{rk.world} subtrees (one per rank), roots merged pairwise into rank 0"
+                                       if rk.world > 1 else "one GPU"),
                        "terms": terms, "levels": levels, "products": products,
                        "root_limbs": {"P": lengths[0], "Q": lengths[1], "T": lengths[2]}},
             "bit_exact_vs_reference_root": exact,
@@ -560,6 +576,68 @@ def run_chudnovsky(args) -> None:
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 4 * sum(lengths),
                     "path": "b2m_chudnovsky_bs + copy of the root to host"},
             "cpu_baseline": cpu, "clocks": clocks}), flush=True)
+    ranks.close(rk)
+
+
+def run_pi(args) -> None:
+    """The digit string of pi for `--digits` digits (default 10^7), every step
+    on one device (b2m_compute_pi): tree, square root, division, decimal
+    conversion. The leading 1,000,000 digits are checked against the
+    reference's own 1,000,000-digit run (tests/golden/pi_digits.json)."""
+    import hashlib
+
+    import torch
+
+    import b200mul
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return  # one product chain, one GPU: other ranks have nothing to do
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    b200mul.init(local)
+    for _ in range(args.warmup):
+        b200mul.compute_pi(min(args.digits, 100000))
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    runs = []
+    for _ in range(args.steps):
+        t = {}
+        s = b200mul.compute_pi(args.digits, t)
+        runs.append(t)
+    clocks = sampler.stop()
+    med = sorted(runs, key=lambda t: t["total_ms"])[len(runs) // 2]
+    checked = None
+    fixture = os.path.join(ROOT, "tests", "golden", "pi_digits.json")
+    if os.path.exists(fixture):
+        ref = {r["digits"]: r for r in json.load(open(fixture))["runs"]}
+        d = max([k for k in ref if k <= args.digits], default=None)
+        if d:
+            checked = {"digits": d, "match": hashlib.sha256(s[: 2 + d].encode()).hexdigest() == ref[d]["sha256"],
+                       "reference_compute_pi_s": ref[d]["ref_s"]}
+    cpu = None
+    if not args.no_cpu_baseline:
+        oracle_mod, kind, _ = _ref_or_port()
+        sample = 100000
+        t0 = time.perf_counter()
+        if kind == "reference":
+            oracle_mod.compute_pi_ref(sample)
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(dt * 1e3, 1), "unit": "ms", "cores": 1, "kind": kind,
+               "sample": f"the reference's compute_pi_chudnovsky({sample}) (NttCpu products, schoolbook "
+                         "division and square root, 1 thread) on this host"} if kind == "reference" else None
+    print(json.dumps({
+        "metric": f"ms per {args.digits}-digit pi string (compute_pi_chudnovsky on the device)",
+        "value": round(med["total_ms"], 1), "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(med["total_ms"], 1), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 limbs / u64 GF(p)", "data": "deterministic: the Chudnovsky series",
+        "config": {"workload": f"compute_pi({args.digits}): tree, isqrt, division, decimal on device",
+                   "terms": med["terms"]},
+        "split_ms": {k: round(med[k], 1) for k in ("tree_ms", "sqrt_ms", "div_ms", "decimal_ms")},
+        "prefix_vs_reference": checked, "cpu_baseline": cpu,
+        "e2e": {"value": round(med["total_ms"], 1), "unit": "ms", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": args.digits + 2, "path": "b2m_compute_pi (C ABI), string in host memory"},
+        "clocks": clocks}), flush=True)
 
 
 def run_serve(args) -> None:
@@ -572,8 +650,12 @@ def run_serve(args) -> None:
 
     import b200mul
 
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    rank = int(os.environ.get("RANK", "0"))
+    import ranks
+
+    # Several GPUs: one server per rank, each with its own arrival stream at
+    # --rate (weak scaling); latencies and throughput gathered to rank 0.
+    rk = ranks.from_env("nccl", timeout_s=600)
+    rank, local = rk.rank, rk.local
     torch.cuda.set_device(local)
     b200mul.init(local)
     rng = np.random.default_rng(2000 + rank)
@@ -625,17 +707,28 @@ def run_serve(args) -> None:
     clocks = sampler.stop()
     st = srv.stats()
     srv.stop()
-    lat = np.array(lat)
     offered_limbs = int(lens.sum())
+    if rk.world > 1:
+        mine = {"lat": lat, "bad": bad, "limbs": limbs_done, "offered": offered_limbs, "wall": wall, "n": n_req}
+        every = [None] * rk.world
+        rk.dist.all_gather_object(every, mine)
+        lat = [x for e in every for x in e["lat"]]
+        bad = sum(e["bad"] for e in every)
+        limbs_done = sum(e["limbs"] for e in every)
+        offered_limbs = sum(e["offered"] for e in every)
+        wall = max(e["wall"] for e in every)
+        n_req = sum(e["n"] for e in every)
+    ranks.close(rk)
+    lat = np.array(lat)
     if rank == 0:
         print(json.dumps({
             "metric": "serve p50/p99 latency ms (Poisson arrivals, log-uniform 2^10..2^24 limbs)",
             "value": round(float(np.percentile(lat, 50)), 2), "unit": "ms",
             "p99_ms": round(float(np.percentile(lat, 99)), 2), "mean_ms": round(float(lat.mean()), 2),
-            "n_gpus": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "n_gpus": rk.world, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "u64 (GF(p), p=2^64-2^32+1)",
             "data": "synthetic: seeded random limbs generated on the device per request",
-            "config": {"workload": f"{args.rate} req/s Poisson for {args.duration} s", "requests": n_req,
+            "config": {"workload": f"{args.rate} req/s Poisson for {args.duration} s per GPU", "requests": n_req,
                        "hbm_budget_gb": args.serve_budget_gb, "streams": args.serve_streams,
                        "max_batch": args.serve_batch, "submit_window_s": round(submit_end, 2)},
             "throughput": {"req_per_s": round(n_req / wall, 1), "glimbs_per_s": round(limbs_done / wall / 1e9, 3),
@@ -651,9 +744,10 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["single", "batch", "chudnovsky", "serve"], default="single",
+    ap.add_argument("--workload", choices=["single", "batch", "chudnovsky", "pi", "serve"], default="single",
                     help="single: the 2^24-limb product (headline); batch: 4096 log-uniform pairs; "
-                         "chudnovsky: the binary-splitting tree; serve: Poisson request stream")
+                         "chudnovsky: the binary-splitting tree; pi: the whole digit string on the device; "
+                         "serve: Poisson request stream")
     ap.add_argument("--digits", type=int, default=10000000)
     ap.add_argument("--rate", type=float, default=2000.0, help="serve: Poisson arrival rate (req/s)")
     ap.add_argument("--duration", type=float, default=10.0, help="serve: seconds of arrivals")
@@ -661,6 +755,8 @@ def main():
     ap.add_argument("--serve-streams", type=int, default=4)
     ap.add_argument("--serve-batch", type=int, default=64)
     ap.add_argument("--batch-jobs", type=int, default=4096)
+    ap.add_argument("--batch-split", action="store_true",
+                    help="batch, several GPUs: partition one batch over the ranks (LPT) instead of one per rank")
     ap.add_argument("--na", type=int, default=NA)
     ap.add_argument("--nb", type=int, default=NB)
     ap.add_argument("--e2e-steps", type=int, default=20)
@@ -676,6 +772,8 @@ def main():
         run_batch(args)
     elif args.workload == "chudnovsky":
         run_chudnovsky(args)
+    elif args.workload == "pi":
+        run_pi(args)
     elif args.workload == "serve":
         run_serve(args)
     else:

@@ -34,7 +34,7 @@ _u64 = ctypes.c_uint64
 STATUS = {
     0: "B2M_OK", 1: "B2M_ERR_INVALID_ARGUMENT", 2: "B2M_ERR_NO_DEVICE", 3: "B2M_ERR_NOT_INITIALIZED",
     4: "B2M_ERR_CUDA", 5: "B2M_ERR_OUT_OF_MEMORY", 6: "B2M_ERR_TOO_LARGE", 7: "B2M_ERR_OUTPUT_TOO_SMALL",
-    8: "B2M_ERR_DEVICE_TIMEOUT", 9: "B2M_ERR_QUEUE_FULL", 10: "B2M_ERR_NOT_FOUND", 11: "B2M_ERR_SHUTDOWN",
+    8: "B2M_ERR_DEVICE_TIMEOUT", 9: "B2M_ERR_QUEUE_FULL", 10: "B2M_ERR_NOT_FOUND", 11: "B2M_ERR_SHUTDOWN", 12: "B2M_ERR_INTERNAL",
 }
 OK, INVALID_ARGUMENT, NO_DEVICE, NOT_INITIALIZED = 0, 1, 2, 3
 CUDA, OUT_OF_MEMORY, TOO_LARGE, OUTPUT_TOO_SMALL, DEVICE_TIMEOUT = 4, 5, 6, 7, 8
@@ -255,6 +255,9 @@ _sig("b2m_pqt_info", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(_u64), ctype
 _sig("b2m_pqt_device", ctypes.c_void_p, [ctypes.c_void_p, ctypes.c_int])
 _sig("b2m_pqt_copy", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _u32p, _u64])
 _sig("b2m_pqt_free", ctypes.c_int, [ctypes.c_void_p])
+_sig("b2m_pqt_merge", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)])
+_sig("b2m_pqt_import", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(_u64), ctypes.c_int32,
+                                      ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)])
 
 
 class PQT:
@@ -301,6 +304,48 @@ def chudnovsky_bs(a: int, b: int, stream: int = 0) -> PQT:
     return PQT(h)
 
 
+def pqt_merge(left: PQT, right: PQT, stream: int = 0) -> PQT:
+    """(P, Q, T) of the union of two adjacent term ranges, left first
+    (reference: the merge step of chudnovsky_bs, src/chudnovsky.cpp:96-100)."""
+    h = ctypes.c_void_p()
+    check(lib.b2m_pqt_merge(left.handle, right.handle, stream or None, ctypes.byref(h)), "b2m_pqt_merge")
+    return PQT(h)
+
+
+def pqt_import(ptrs, lengths, t_sign: int, stream: int = 0) -> PQT:
+    """A node copied from device limbs: ptrs/lengths of P, Q, |T| and T's sign."""
+    p = (ctypes.c_void_p * 3)(*[int(x) if x else None for x in ptrs])
+    ln = (_u64 * 3)(*[int(x) for x in lengths])
+    h = ctypes.c_void_p()
+    check(lib.b2m_pqt_import(p, ln, int(t_sign), stream or None, ctypes.byref(h)), "b2m_pqt_import")
+    return PQT(h)
+
+
+_sig("b2m_divmod_device", ctypes.c_int, [ctypes.c_void_p, _u64, ctypes.c_void_p, _u64, ctypes.c_void_p, _u64,
+                                         ctypes.POINTER(_u64), ctypes.c_void_p, _u64, ctypes.POINTER(_u64),
+                                         ctypes.c_void_p])
+_sig("b2m_isqrt_device", ctypes.c_int, [ctypes.c_void_p, _u64, ctypes.c_void_p, _u64, ctypes.POINTER(_u64),
+                                        ctypes.c_void_p])
+
+
+def divmod_device(d_a: int, na: int, d_b: int, nb: int, d_q: int, q_cap: int, d_r: int, r_cap: int,
+                  stream: int = 0):
+    """Reference: divmod_knuth / div_fast (src/bignum_div.cpp:162-178), on the
+    device. Returns the trimmed lengths (q_len, r_len)."""
+    ql, rl = _u64(0), _u64(0)
+    check(lib.b2m_divmod_device(d_a or None, na, d_b, nb, d_q or None, q_cap, ctypes.byref(ql), d_r or None,
+                                r_cap, ctypes.byref(rl), stream or None), "b2m_divmod_device")
+    return int(ql.value), int(rl.value)
+
+
+def isqrt_device(d_a: int, na: int, d_out: int, cap: int, stream: int = 0) -> int:
+    """Reference: isqrt (src/bignum_div.cpp:189-204), on the device. Returns
+    the trimmed length of floor(sqrt(a))."""
+    n = _u64(0)
+    check(lib.b2m_isqrt_device(d_a or None, na, d_out, cap, ctypes.byref(n), stream or None), "b2m_isqrt_device")
+    return int(n.value)
+
+
 DIGITS_PER_TERM = 14.181647462725477  # src/chudnovsky.cpp:46
 
 
@@ -314,38 +359,38 @@ def _to_int(limbs: np.ndarray) -> int:
     return int.from_bytes(np.ascontiguousarray(limbs, dtype="<u4").tobytes(), "little")
 
 
+class PiTimings(ctypes.Structure):
+    _fields_ = [("tree_ms", ctypes.c_double), ("sqrt_ms", ctypes.c_double), ("div_ms", ctypes.c_double),
+                ("decimal_ms", ctypes.c_double), ("total_ms", ctypes.c_double), ("terms", _u64)]
+
+
+_sig("b2m_to_decimal_device", ctypes.c_int, [ctypes.c_void_p, _u64, ctypes.c_char_p, _u64, ctypes.POINTER(_u64),
+                                             ctypes.c_void_p])
+_sig("b2m_compute_pi", ctypes.c_int, [_u64, ctypes.c_char_p, _u64, ctypes.POINTER(_u64), ctypes.POINTER(PiTimings)])
+
+
+def to_decimal_device(d_a: int, na: int, stream: int = 0) -> str:
+    """Reference: BigInt::to_decimal (src/bignum_div.cpp:239-267), on the device."""
+    cap = int(na * 32 * 0.30103) + 16
+    buf = ctypes.create_string_buffer(cap)
+    n = _u64(0)
+    check(lib.b2m_to_decimal_device(d_a or None, na, buf, cap, ctypes.byref(n), stream or None),
+          "b2m_to_decimal_device")
+    return buf.raw[: n.value].decode()
+
+
 def compute_pi(digits: int, timings: dict | None = None) -> str:
-    """Reference: compute_pi_chudnovsky (src/chudnovsky.cpp:107-164).
-
-    Same guard digits, term count, isqrt of 10005 * 10^(2 prec), floor
-    division and formatting; the binary-splitting tree runs on the device
-    (b2m_chudnovsky_bs) and the final assembly uses exact host integers."""
-    import math
-    import sys
-    import time
-
-    if hasattr(sys, "set_int_max_str_digits"):
-        sys.set_int_max_str_digits(0)
-    prec = digits + 16
-    n = chudnovsky_terms_for_digits(prec)
-    t0 = time.perf_counter()
-    r = chudnovsky_bs(0, n)
-    q = _to_int(r.limbs(1))
-    t = _to_int(r.limbs(2))
-    sign = r.t_sign
-    r.free()
-    t1 = time.perf_counter()
-    one = 10 ** prec
-    sqrt_c = math.isqrt(10005 * one * one)
-    numerator = q * 426880 * sqrt_c
-    pi_scaled = numerator // (t if sign > 0 else -t)
-    s = str(pi_scaled)
-    t2 = time.perf_counter()
+    """Reference: compute_pi_chudnovsky (src/chudnovsky.cpp:107-164), every
+    step on the device (b2m_compute_pi): tree, square root, division and
+    decimal conversion. Returns "3." and `digits` digits."""
+    buf = ctypes.create_string_buffer(digits + 8)
+    n = _u64(0)
+    t = PiTimings()
+    check(lib.b2m_compute_pi(digits, buf, len(buf), ctypes.byref(n), ctypes.byref(t)), "b2m_compute_pi")
     if timings is not None:
-        timings.update({"terms": n, "tree_s": t1 - t0, "assembly_s": t2 - t1})
-    if digits == 0:
-        return "3"
-    return s[0] + "." + s[1:1 + digits]
+        timings.update({"terms": int(t.terms), "tree_ms": t.tree_ms, "sqrt_ms": t.sqrt_ms, "div_ms": t.div_ms,
+                        "decimal_ms": t.decimal_ms, "total_ms": t.total_ms})
+    return buf.raw[: n.value].decode()
 
 
 # ---- serving ------------------------------------------------------------------------

@@ -213,6 +213,7 @@ const char* b2m_strerror(b2m_status s) {
         case B2M_ERR_QUEUE_FULL: return "request table full";
         case B2M_ERR_NOT_FOUND: return "unknown ticket";
         case B2M_ERR_SHUTDOWN: return "server stopping";
+        case B2M_ERR_INTERNAL: return "internal check failed";
     }
     return "unknown status";
 }

@@ -28,6 +28,7 @@
 #include "b2m.h"
 #include "b2m_context.h"
 #include "b2m_internal.h"
+#include "gp_scan.cuh"
 
 namespace b2m {
 
@@ -216,40 +217,6 @@ __global__ void k_bs_zero_ws(const ProdJob* __restrict__ jobs, u64 njobs, u64 sc
 }
 
 // ---------------------------------------------------------------------------- T = sx*X + sy*Y
-// Binary carry (or borrow) of a group of limbs as (generate, propagate).
-struct GP {
-    u32 g, p;
-};
-__device__ __forceinline__ GP gp_then(GP lo, GP hi) { return {hi.g | (hi.p & lo.g), hi.p & lo.p}; }
-
-constexpr int ADD_LPT = 8;  // limbs per thread
-
-// Exclusive block scan of GP (low threads first). blockDim multiple of 32.
-__device__ __forceinline__ GP block_scan_gp(GP v, GP* ws, GP* total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    GP inc = v;
-    for (int off = 1; off < 32; off <<= 1) {
-        GP o{__shfl_up_sync(0xFFFFFFFFu, inc.g, off), __shfl_up_sync(0xFFFFFFFFu, inc.p, off)};
-        if (lane >= off) inc = gp_then(o, inc);
-    }
-    GP ex{__shfl_up_sync(0xFFFFFFFFu, inc.g, 1), __shfl_up_sync(0xFFFFFFFFu, inc.p, 1)};
-    if (lane == 0) ex = {0, 1};
-    if (lane == 31) ws[warp] = inc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        GP acc{0, 1};
-        for (int w = 0; w < nw; ++w) {
-            GP t = ws[w];
-            ws[w] = acc;
-            acc = gp_then(acc, t);
-        }
-        ws[nw] = acc;
-    }
-    __syncthreads();
-    *total = ws[nw];
-    return gp_then(ws[warp], ex);
-}
-
 // One CTA per merge: T' = sign(TL)*X + sign(TR)*Y (X = TL*QR, Y = PL*TR).
 __global__ void k_bs_signed_add(const ScratchXY S, const int* __restrict__ sign_l, LevelView Ln, u64 m2) {
     __shared__ GP s_ws[33];
@@ -554,9 +521,135 @@ static cudaError_t merge_level(Context* c, const LevelView& L, const uint64_t mx
     return e;
 }
 
+// Wraps a finished one-node level into a b2m_pqt (takes ownership of mem).
+static b2m_status finish_pqt(Context* c, const LevelView& L, void* mem, uint64_t bytes, uint32_t levels,
+                             uint64_t products, cudaStream_t s, b2m_pqt** out) {
+    cudaError_t e = cudaStreamSynchronize(s);
+    b2m_status st = e == cudaSuccess ? take_device_error(c) : cuda_status(e, "binary splitting");
+    u64 hl[3] = {0, 0, 0};
+    int hs = 0;
+    if (st == B2M_OK) {
+        e = cudaMemcpy(hl, L.len, sizeof(hl), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(&hs, L.sign, sizeof(int), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) st = cuda_status(e, "cudaMemcpy(pqt lengths)");
+    }
+    if (st != B2M_OK) {
+        cudaFreeAsync(mem, s);
+        cudaStreamSynchronize(s);
+        budget_release(c, bytes);
+        return st;
+    }
+    b2m_pqt* r = new b2m_pqt();
+    r->ctx = c;
+    r->mem = mem;
+    r->bytes = bytes;
+    r->root = L;
+    r->levels = levels;
+    r->products = products;
+    for (int f = 0; f < 3; ++f) r->host_len[f] = hl[f];
+    r->host_sign = hs;
+    *out = r;
+    return B2M_OK;
+}
+
+// A level of m nodes filled from device limbs: node i of family f is
+// src[i][f] (len[i][f] limbs), signs sg[i]; the rest of each slot is zero.
+static cudaError_t level_from(Context* c, int m, const uint32_t* const src[][3], const uint64_t len[][3],
+                              const int sg[], LevelView* L, void** mem, uint64_t* bytes, cudaStream_t s) {
+    uint64_t stride[3] = {1, 1, 1};
+    for (int i = 0; i < m; ++i)
+        for (int f = 0; f < 3; ++f) stride[f] = std::max(stride[f], len[i][f]);
+    cudaError_t e = alloc_level(c, (uint64_t)m, stride, L, mem, bytes, s);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(*mem, 0, *bytes, s)) != cudaSuccess) return e;
+    u64 hl[6];
+    for (int i = 0; i < m; ++i)
+        for (int f = 0; f < 3; ++f) {
+            hl[f * m + i] = len[i][f];
+            if (len[i][f] && (e = cudaMemcpyAsync(L->limbs[f] + i * stride[f], src[i][f], len[i][f] * 4,
+                                                  cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+                return e;
+        }
+    if ((e = cudaMemcpyAsync(L->len, hl, 3 * m * sizeof(u64), cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(L->sign, sg, m * sizeof(int), cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+    return cudaStreamSynchronize(s);  // the host arrays above are on this frame
+}
+
 }  // namespace b2m
 
 extern "C" {
+
+b2m_status b2m_pqt_import(const uint32_t* const d_limbs[3], const uint64_t len[3], int32_t t_sign,
+                          b2m_stream stream, b2m_pqt** result) {
+    Context* c = ctx();
+    if (!c) return B2M_ERR_NOT_INITIALIZED;
+    if (!result || !d_limbs || !len) return B2M_ERR_INVALID_ARGUMENT;
+    for (int f = 0; f < 3; ++f)
+        if (len[f] && !d_limbs[f]) return B2M_ERR_INVALID_ARGUMENT;
+    if (t_sign < -1 || t_sign > 1) return B2M_ERR_INVALID_ARGUMENT;
+    *result = nullptr;
+    cudaSetDevice(c->device);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const uint32_t* src[1][3] = {{d_limbs[0], d_limbs[1], d_limbs[2]}};
+    const uint64_t ln[1][3] = {{len[0], len[1], len[2]}};
+    const int sg[1] = {t_sign};
+    LevelView L{};
+    void* mem = nullptr;
+    uint64_t bytes = 0;
+    cudaError_t e = level_from(c, 1, src, ln, sg, &L, &mem, &bytes, s);
+    if (e != cudaSuccess) {
+        if (mem) {
+            cudaFreeAsync(mem, s);
+            cudaStreamSynchronize(s);
+            budget_release(c, bytes);
+        }
+        return cuda_status(e, "b2m_pqt_import");
+    }
+    return finish_pqt(c, L, mem, bytes, 0, 0, s, result);
+}
+
+b2m_status b2m_pqt_merge(const b2m_pqt* left, const b2m_pqt* right, b2m_stream stream, b2m_pqt** result) {
+    Context* c = ctx();
+    if (!c) return B2M_ERR_NOT_INITIALIZED;
+    if (!left || !right || !result) return B2M_ERR_INVALID_ARGUMENT;
+    *result = nullptr;
+    cudaSetDevice(c->device);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const uint32_t* src[2][3];
+    uint64_t ln[2][3];
+    int sg[2] = {left->host_sign, right->host_sign};
+    for (int f = 0; f < 3; ++f) {
+        src[0][f] = left->root.limbs[f];
+        src[1][f] = right->root.limbs[f];
+        ln[0][f] = left->host_len[f];
+        ln[1][f] = right->host_len[f];
+    }
+    LevelView L{};
+    void* mem = nullptr;
+    uint64_t bytes = 0;
+    cudaError_t e = level_from(c, 2, src, ln, sg, &L, &mem, &bytes, s);
+    LevelView Ln{};
+    void* mem_n = nullptr;
+    uint64_t bytes_n = 0, products = left->products + right->products;
+    if (e == cudaSuccess) {
+        const uint64_t mx[3] = {std::max(ln[0][0], ln[1][0]), std::max(ln[0][1], ln[1][1]),
+                                std::max(ln[0][2], ln[1][2])};
+        e = merge_level(c, L, mx, &Ln, &mem_n, &bytes_n, &products, s);
+    }
+    if (mem) {
+        cudaFreeAsync(mem, s);
+        budget_release(c, bytes);
+    }
+    if (e != cudaSuccess) {
+        if (mem_n) {
+            cudaFreeAsync(mem_n, s);
+            budget_release(c, bytes_n);
+        }
+        cudaStreamSynchronize(s);
+        return cuda_status(e, "b2m_pqt_merge");
+    }
+    return finish_pqt(c, Ln, mem_n, bytes_n, std::max(left->levels, right->levels) + 1, products, s, result);
+}
 
 b2m_status b2m_chudnovsky_bs(uint64_t a, uint64_t b, b2m_stream stream, b2m_pqt** out) {
     Context* c = ctx();
@@ -572,8 +665,7 @@ b2m_status b2m_chudnovsky_bs(uint64_t a, uint64_t b, b2m_stream stream, b2m_pqt*
     unsigned long long* d_tmp = nullptr;
     cudaError_t e = cudaMallocAsync(&d_tmp, 64, s);
     if (e != cudaSuccess) return cuda_status(e, "cudaMallocAsync");
-    b2m_pqt* r = new b2m_pqt();
-    r->ctx = c;
+    uint64_t products = 0;
     const uint64_t stride0[3] = {4, 4, 4};
     LevelView L{};
     void* mem = nullptr;
@@ -590,7 +682,7 @@ b2m_status b2m_chudnovsky_bs(uint64_t a, uint64_t b, b2m_stream stream, b2m_pqt*
         LevelView Ln{};
         void* mem_n = nullptr;
         uint64_t bytes_n = 0;
-        e = merge_level(c, L, mx, &Ln, &mem_n, &bytes_n, &r->products, s);
+        e = merge_level(c, L, mx, &Ln, &mem_n, &bytes_n, &products, s);
         if (e == cudaSuccess) e = level_maxlen(Ln, d_tmp, mx, s);
         if (mem) {
             cudaFreeAsync(mem, s);
@@ -602,36 +694,15 @@ b2m_status b2m_chudnovsky_bs(uint64_t a, uint64_t b, b2m_stream stream, b2m_pqt*
         ++levels;
     }
     cudaFreeAsync(d_tmp, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         if (mem) {
             cudaFreeAsync(mem, s);
             cudaStreamSynchronize(s);
             budget_release(c, bytes);
         }
-        delete r;
         return cuda_status(e, "binary splitting");
     }
-    b2m_status st = take_device_error(c);
-    if (st != B2M_OK) {
-        cudaFreeAsync(mem, s);
-        cudaStreamSynchronize(s);
-        budget_release(c, bytes);
-        delete r;
-        return st;
-    }
-    r->mem = mem;
-    r->bytes = bytes;
-    r->root = L;
-    r->levels = levels;
-    u64 hl[3];
-    int hs = 0;
-    cudaMemcpy(hl, L.len, sizeof(hl), cudaMemcpyDeviceToHost);
-    cudaMemcpy(&hs, L.sign, sizeof(int), cudaMemcpyDeviceToHost);
-    for (int f = 0; f < 3; ++f) r->host_len[f] = hl[f];
-    r->host_sign = hs;
-    *out = r;
-    return B2M_OK;
+    return finish_pqt(c, L, mem, bytes, levels, products, s, out);
 }
 
 b2m_status b2m_pqt_info(const b2m_pqt* r, uint64_t len[3], int32_t* t_sign, uint32_t* levels, uint64_t* products) {

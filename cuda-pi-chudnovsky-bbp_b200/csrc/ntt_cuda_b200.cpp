@@ -36,3 +36,46 @@ std::vector<uint32_t> mul_ntt_cuda(const std::vector<uint32_t>& a, const std::ve
 }
 
 }  // namespace pidigits
+
+// Vector forms of the sub-quadratic division, square root and decimal
+// conversion, for the seams the reference leaves for them: the body of
+// div_fast (src/bignum_div.cpp:170-178), of isqrt (:189-204) and of
+// BigInt::to_decimal (:239-267) can forward the magnitudes here (signs stay
+// with the caller; all three take non-negative values). They throw on failure
+// like mul_ntt_cuda.
+namespace pidigits_b200 {
+
+static void check(b2m_status s, const char* what) {
+    if (s != B2M_OK)
+        throw std::runtime_error(std::string(what) + ": " + b2m_strerror(s) + " (" + b2m_last_error() + ")");
+}
+
+std::vector<uint32_t> div_floor(const std::vector<uint32_t>& a, const std::vector<uint32_t>& b,
+                                std::vector<uint32_t>* rem) {
+    std::vector<uint32_t> q(a.size() >= b.size() ? a.size() - b.size() + 1 : 1), r(b.size());
+    uint64_t ql = 0, rl = 0;
+    check(b2m_divmod_host(a.data(), a.size(), b.data(), b.size(), q.data(), q.size(), &ql, r.data(), r.size(), &rl),
+          "div_floor");
+    q.resize(ql);
+    r.resize(rl);
+    if (rem) *rem = std::move(r);
+    return q;
+}
+
+std::vector<uint32_t> isqrt(const std::vector<uint32_t>& a) {
+    std::vector<uint32_t> s((a.size() + 1) / 2 + 1);
+    uint64_t n = 0;
+    check(b2m_isqrt_host(a.data(), a.size(), s.data(), s.size(), &n), "isqrt");
+    s.resize(n);
+    return s;
+}
+
+std::string to_decimal(const std::vector<uint32_t>& a) {
+    std::string out((size_t)(a.size() * 9.64) + 16, '\0');  // 32 log10(2) < 9.64 digits per limb
+    uint64_t n = 0;
+    check(b2m_to_decimal_host(a.data(), a.size(), &out[0], out.size(), &n), "to_decimal");
+    out.resize(n);
+    return out;
+}
+
+}  // namespace pidigits_b200

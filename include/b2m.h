@@ -49,7 +49,8 @@ typedef enum b2m_status {
     B2M_ERR_DEVICE_TIMEOUT = 8,    /* a bounded device-side wait gave up (carry lookback) */
     B2M_ERR_QUEUE_FULL = 9,        /* serving: request table full */
     B2M_ERR_NOT_FOUND = 10,        /* serving: unknown ticket */
-    B2M_ERR_SHUTDOWN = 11          /* serving: the server is stopping */
+    B2M_ERR_SHUTDOWN = 11,         /* serving: the server is stopping */
+    B2M_ERR_INTERNAL = 12          /* an exact-arithmetic check failed (a library bug; detail: b2m_last_error) */
 } b2m_status;
 
 /* ---- lifetime ------------------------------------------------------------ */
@@ -185,6 +186,74 @@ const uint32_t* b2m_pqt_device(const b2m_pqt* r, int which);
 b2m_status b2m_pqt_copy(const b2m_pqt* r, int which, uint32_t* host, uint64_t cap);
 
 b2m_status b2m_pqt_free(b2m_pqt* r);
+
+/* (P, Q, T) of [a, c) from those of the adjacent ranges [a, b) (left) and
+ * [b, c) (right): P = Pl*Pr, Q = Ql*Qr, T = Tl*Qr + Pl*Tr -- the merge step of
+ * chudnovsky_bs (src/chudnovsky.cpp:96-100), one tree level of two nodes on
+ * the device. Inputs are unchanged. Lets a tree be split into subtrees (on
+ * several GPUs) and merged at the top. */
+b2m_status b2m_pqt_merge(const b2m_pqt* left, const b2m_pqt* right, b2m_stream stream, b2m_pqt** result);
+
+/* A node made from device limbs, copied (the caller keeps its buffers):
+ * P, Q and |T| of len[0..2] trimmed limbs at d_limbs[0..2] (on this device),
+ * and the sign of T (-1, 0, 1) -- e.g. a subtree root received from another
+ * GPU. No reference counterpart (the reference has one process, one GPU). */
+b2m_status b2m_pqt_import(const uint32_t* const d_limbs[3], const uint64_t len[3], int32_t t_sign,
+                          b2m_stream stream, b2m_pqt** result);
+
+/* ---- division, square root, decimal -------------------------------------------------
+ * The big-integer steps after the tree in compute_pi_chudnovsky
+ * (src/chudnovsky.cpp:107-164), on the device and sub-quadratic: the
+ * reference's are schoolbook (div_fast forwards to divmod_knuth,
+ * src/bignum_div.cpp:162-178; isqrt is Newton with a Knuth division per step,
+ * :189-204; to_decimal divides by 10^9 repeatedly, :239-267). Results are the
+ * same integers: Newton reciprocals and roots only seed estimates that an
+ * exact correction against the remainder finishes. Operands are device
+ * magnitudes (leading zero limbs allowed); calls are synchronous on `stream`
+ * and write the trimmed lengths to host memory. */
+
+/* q = floor(a / b), r = a mod b (b != 0). d_q / d_r may be NULL when not
+ * wanted; q needs q_cap >= na - nb + 1 limbs, r needs r_cap >= nb. */
+b2m_status b2m_divmod_device(const uint32_t* d_a, uint64_t na, const uint32_t* d_b, uint64_t nb,
+                             uint32_t* d_q, uint64_t q_cap, uint64_t* q_len,
+                             uint32_t* d_r, uint64_t r_cap, uint64_t* r_len, b2m_stream stream);
+
+/* floor(sqrt(a)); out needs cap >= (na + 1) / 2 limbs. */
+b2m_status b2m_isqrt_device(const uint32_t* d_a, uint64_t na, uint32_t* d_out, uint64_t cap, uint64_t* out_len,
+                            b2m_stream stream);
+
+/* Decimal digits of a, no leading zeros ("0" for zero), NUL-terminated into
+ * the host buffer out (cap >= digits + 1); *len = digits. Divide and conquer
+ * by 10^(9 2^j), each level's divisions batched. */
+b2m_status b2m_to_decimal_device(const uint32_t* d_a, uint64_t na, char* out, uint64_t cap, uint64_t* len,
+                                 b2m_stream stream);
+
+/* The same three with host buffers, synchronous on the legacy default
+ * stream: the shapes the reference's BigInt functions need (a, b, q, r and
+ * out are host limb arrays; out of b2m_to_decimal_host is a host char
+ * buffer). */
+b2m_status b2m_divmod_host(const uint32_t* a, uint64_t na, const uint32_t* b, uint64_t nb, uint32_t* q,
+                           uint64_t q_cap, uint64_t* q_len, uint32_t* r, uint64_t r_cap, uint64_t* r_len);
+b2m_status b2m_isqrt_host(const uint32_t* a, uint64_t na, uint32_t* out, uint64_t cap, uint64_t* out_len);
+b2m_status b2m_to_decimal_host(const uint32_t* a, uint64_t na, char* out, uint64_t cap, uint64_t* len);
+
+/* Wall-clock split of b2m_compute_pi (milliseconds). */
+typedef struct b2m_pi_timings {
+    double tree_ms;      /* binary splitting to (P, Q, T) */
+    double sqrt_ms;      /* 10^prec and floor(sqrt(10005 * 10^(2 prec))) */
+    double div_ms;       /* numerator and the floor division by T */
+    double decimal_ms;   /* decimal conversion */
+    double total_ms;
+    uint64_t terms;
+} b2m_pi_timings;
+
+/* Replaces compute_pi_chudnovsky (src/chudnovsky.cpp:107-164) with every
+ * step on this GPU: "3." followed by `digits` digits of pi, NUL-terminated,
+ * into out (cap >= digits + 3); *len = string length. Same guard digits,
+ * term count and integer steps as the reference, so the same string.
+ * Term indices stay below 2,000,000 (about 28 million digits). times may
+ * be NULL. Uses the legacy default stream. */
+b2m_status b2m_compute_pi(uint64_t digits, char* out, uint64_t cap, uint64_t* len, b2m_pi_timings* times);
 
 /* ---- serving ---------------------------------------------------------------------
  * No counterpart in the reference. A continuous-batching multiply server:

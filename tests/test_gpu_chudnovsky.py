@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 import oracle
+import ranks
 from golden_util import sha_limbs
 
 pytestmark = pytest.mark.gpu
@@ -50,3 +51,44 @@ def test_compute_pi_matches_reference_digits(b2m_gpu, digits):
     s = b2m_gpu.compute_pi(digits)
     assert s[:102] == runs[digits]["head"]
     assert hashlib.sha256(s.encode()).hexdigest() == runs[digits]["sha256"]
+
+
+@pytest.mark.parametrize("digits", [1000, 100000, 1000000])
+def test_split_and_merged_trees_equal_the_reference_root(b2m_gpu, digits):
+    """The tree split into subtrees (as ranks.py splits it over GPUs) and
+    merged with b2m_pqt_merge, subtree roots moved through b2m_pqt_import on
+    the way, equals the reference's root."""
+    tr = next(t for t in json.load(open(os.path.join(GOLD, "chudnovsky.json")))["trees"] if t["digits"] == digits)
+    n = tr["terms"]
+    for world in (2, 3, 8):
+        nodes = []
+        for a, b in ranks.term_ranges(n, world):
+            r = b2m_gpu.chudnovsky_bs(a, b)
+            moved = b2m_gpu.pqt_import([b2m_gpu.lib.b2m_pqt_device(r.handle, f) for f in range(3)],
+                                       r.lengths, r.t_sign)
+            r.free()
+            nodes.append(moved)
+        # the same pairwise order as ranks.merge_schedule
+        held = dict(enumerate(nodes))
+        for step in ranks.merge_schedule(world):
+            for dst, src in step:
+                m = b2m_gpu.pqt_merge(held[dst], held[src])
+                held[dst].free()
+                held.pop(src).free()
+                held[dst] = m
+        root = held[0]
+        for which, nm in enumerate("PQT"):
+            assert root.lengths[which] == tr[nm]["len"], (world, nm)
+            assert sha_limbs(root.limbs(which)) == tr[nm]["sha256"], (world, nm)
+        assert root.t_sign == tr["T"]["sign"]
+        root.free()
+
+
+def test_pqt_merge_small_ranges_match_oracle(b2m_gpu):
+    for a, b, c in [(0, 1, 2), (0, 5, 9), (3, 4, 40), (10, 200, 201)]:
+        left, right = b2m_gpu.chudnovsky_bs(a, b), b2m_gpu.chudnovsky_bs(b, c)
+        m = b2m_gpu.pqt_merge(left, right)
+        for (sg, mg), (sw, mw) in zip(m.signed(), oracle.bs_port(a, c)):
+            assert sg == sw and np.array_equal(mg, mw)
+        for x in (left, right, m):
+            x.free()
