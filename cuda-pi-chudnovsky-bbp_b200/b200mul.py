@@ -369,6 +369,46 @@ _sig("b2m_to_decimal_device", ctypes.c_int, [ctypes.c_void_p, _u64, ctypes.c_cha
 _sig("b2m_compute_pi", ctypes.c_int, [_u64, ctypes.c_char_p, _u64, ctypes.POINTER(_u64), ctypes.POINTER(PiTimings)])
 
 
+_sig("b2m_divmod_host", ctypes.c_int, [_u32p, _u64, _u32p, _u64, _u32p, _u64, ctypes.POINTER(_u64), _u32p, _u64,
+                                       ctypes.POINTER(_u64)])
+_sig("b2m_isqrt_host", ctypes.c_int, [_u32p, _u64, _u32p, _u64, ctypes.POINTER(_u64)])
+_sig("b2m_to_decimal_host", ctypes.c_int, [_u32p, _u64, ctypes.c_char_p, _u64, ctypes.POINTER(_u64)])
+
+
+def _u32_arr(x) -> np.ndarray:
+    return np.ascontiguousarray(x, dtype=np.uint32)
+
+
+def divmod_host(a, b):
+    """Host-limb floor division (b2m_divmod_host): (q, r) as u32 arrays."""
+    a, b = _u32_arr(a), _u32_arr(b)
+    q = np.zeros(max(1, a.size - b.size + 1), np.uint32)
+    r = np.zeros(max(1, b.size), np.uint32)
+    ql, rl = _u64(0), _u64(0)
+    check(lib.b2m_divmod_host(a.ctypes.data_as(_u32p), a.size, b.ctypes.data_as(_u32p), b.size,
+                              q.ctypes.data_as(_u32p), q.size, ctypes.byref(ql), r.ctypes.data_as(_u32p), r.size,
+                              ctypes.byref(rl)), "b2m_divmod_host")
+    return q[: ql.value], r[: rl.value]
+
+
+def isqrt_host(a):
+    a = _u32_arr(a)
+    s = np.zeros((a.size + 1) // 2 + 1, np.uint32)
+    n = _u64(0)
+    check(lib.b2m_isqrt_host(a.ctypes.data_as(_u32p), a.size, s.ctypes.data_as(_u32p), s.size, ctypes.byref(n)),
+          "b2m_isqrt_host")
+    return s[: n.value]
+
+
+def to_decimal_host(a) -> str:
+    a = _u32_arr(a)
+    cap = int(a.size * 9.64) + 16
+    buf = ctypes.create_string_buffer(cap)
+    n = _u64(0)
+    check(lib.b2m_to_decimal_host(a.ctypes.data_as(_u32p), a.size, buf, cap, ctypes.byref(n)), "b2m_to_decimal_host")
+    return buf.raw[: n.value].decode()
+
+
 def to_decimal_device(d_a: int, na: int, stream: int = 0) -> str:
     """Reference: BigInt::to_decimal (src/bignum_div.cpp:239-267), on the device."""
     cap = int(na * 32 * 0.30103) + 16

@@ -160,3 +160,20 @@ def test_compute_pi_short_strings(b2m_gpu):
     assert b2m_gpu.compute_pi(0) == "3"
     for d in (1, 2, 5, 50, 100):
         assert b2m_gpu.compute_pi(d) == head[: 2 + d]
+
+
+def test_host_buffer_forms(b2m_gpu):
+    """b2m_divmod_host / b2m_isqrt_host / b2m_to_decimal_host: the shapes the
+    reference's BigInt seams (div_fast, isqrt, to_decimal) would call."""
+    import math
+    import sys
+
+    sys.set_int_max_str_digits(0)
+    rng = random.Random(11)
+    for na, nb in [(1, 1), (50, 7), (3000, 1000)]:
+        a, b = rand_int(rng, na), rand_int(rng, nb, 9)
+        q, r = b2m_gpu.divmod_host(to_limbs(a), to_limbs(b))
+        assert (to_int(q), to_int(r)) == divmod(a, b)
+        assert to_int(b2m_gpu.isqrt_host(to_limbs(a))) == math.isqrt(a)
+        assert b2m_gpu.to_decimal_host(to_limbs(a)) == str(a)
+    assert b2m_gpu.to_decimal_host(np.zeros(3, np.uint32)) == "0"
