@@ -187,6 +187,40 @@ def plan_describe(na: int, nb: int) -> dict:
             "logc": list(d.logc)[: max(d.npass, 1)], "launches": d.launches}
 
 
+class TuneEntry(ctypes.Structure):
+    _fields_ = [("plan", PlanDesc), ("ms", ctypes.c_float), ("chosen", ctypes.c_uint32)]
+
+
+_sig("b2m_autotune", ctypes.c_int, [_u64, _u64, ctypes.c_void_p, ctypes.POINTER(TuneEntry), ctypes.c_uint32,
+                                    ctypes.POINTER(ctypes.c_uint32)])
+
+
+def autotune(na: int, nb: int, stream: int = 0) -> list[dict]:
+    """Times every candidate plan for an na x nb product and keeps the
+    fastest for that transform length (b2m_autotune). Returns the timings."""
+    out = (TuneEntry * 64)()
+    n = ctypes.c_uint32(0)
+    check(lib.b2m_autotune(na, nb, stream or None, out, 64, ctypes.byref(n)), "b2m_autotune")
+    res = []
+    for e in out[: n.value]:
+        k = max(e.plan.npass, 1)
+        res.append({"logr": list(e.plan.logr)[:k], "logc": list(e.plan.logc)[:k], "ms": round(e.ms, 4),
+                    "chosen": bool(e.chosen)})
+    return res
+
+
+_sig("b2m_set_plan", ctypes.c_int, [ctypes.POINTER(PlanDesc)])
+
+
+def set_plan(ntt_log2: int, logr, logc) -> None:
+    """Fixes the plan of one transform length (b2m_set_plan)."""
+    d = PlanDesc()
+    d.ntt_log2, d.npass = ntt_log2, len(logr) if ntt_log2 > 13 else 0
+    for k, (r, c) in enumerate(zip(logr, logc)):
+        d.logr[k], d.logc[k] = r, c
+    check(lib.b2m_set_plan(ctypes.byref(d)), "b2m_set_plan")
+
+
 def mul_device_traced(a_ptr: int, na: int, b_ptr: int, nb: int, out_ptr: int, out_cap: int,
                       out_len_ptr: int = 0, stream: int = 0) -> list[tuple[str, int, float]]:
     """Device product with per-launch CUDA-event times: [(kind, logr, ms), ...]."""

@@ -7,6 +7,8 @@
 // and status codes instead of a fallback.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -243,7 +245,7 @@ b2m_status b2m_mul_device(const uint32_t* d_a, uint64_t na, const uint32_t* d_b,
     b2m_status st = check_sizes(na, nb, &logn);
     if (st != B2M_OK) return st;
     cudaSetDevice(c->device);
-    const Plan p = make_plan(logn);
+    const Plan p = plan_for(c, logn);
     const uint64_t wsb = workspace_bytes_for(logn);
     if (!budget_reserve(c, wsb)) {
         set_error("HBM budget exhausted");
@@ -267,7 +269,8 @@ b2m_status b2m_plan_describe(uint64_t na, uint64_t nb, b2m_plan_desc* d) {
     int logn;
     b2m_status st = check_sizes(na, nb, &logn);
     if (st != B2M_OK) return st;
-    const Plan p = make_plan(logn);
+    Context* c = ctx();
+    const Plan p = c ? plan_for(c, logn) : make_plan(logn);
     d->ntt_log2 = (uint32_t)logn;
     d->npass = (uint32_t)p.npass;
     for (int k = 0; k < 3; ++k) {
@@ -275,6 +278,108 @@ b2m_status b2m_plan_describe(uint64_t na, uint64_t nb, b2m_plan_desc* d) {
         d->logc[k] = (uint32_t)p.logc[k];
     }
     d->launches = (uint32_t)plan_launches(p);
+    return B2M_OK;
+}
+
+b2m_status b2m_set_plan(const b2m_plan_desc* desc) {
+    Context* c = ctx();
+    if (!c) return B2M_ERR_NOT_INITIALIZED;
+    if (!desc || desc->ntt_log2 < 2 || desc->ntt_log2 > (uint32_t)MAX_LOGN) return B2M_ERR_INVALID_ARGUMENT;
+    const int logn = (int)desc->ntt_log2;
+    // only plans the library can launch: one of the autotuner's candidates
+    for (const Plan& p : plan_candidates(logn)) {
+        bool same = p.npass == (int)desc->npass;
+        for (int k = 0; same && k < p.npass; ++k)
+            same = p.logr[k] == (int)desc->logr[k] && p.logc[k] == (int)desc->logc[k];
+        if (same) {
+            set_tuned(c, logn, p);
+            return B2M_OK;
+        }
+    }
+    set_error("b2m_set_plan: not one of the candidate plans for this length");
+    return B2M_ERR_INVALID_ARGUMENT;
+}
+
+b2m_status b2m_autotune(uint64_t na, uint64_t nb, b2m_stream stream, b2m_tune_entry* out, uint32_t cap,
+                        uint32_t* n) {
+    Context* c = ctx();
+    if (!c) return B2M_ERR_NOT_INITIALIZED;
+    if (na == 0 || nb == 0 || (cap && !out)) return B2M_ERR_INVALID_ARGUMENT;
+    int logn;
+    b2m_status st = check_sizes(na, nb, &logn);
+    if (st != B2M_OK) return st;
+    cudaSetDevice(c->device);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const std::vector<Plan> cands = plan_candidates(logn);
+    auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
+    const uint64_t ba = al(4 * na), bb = al(4 * nb), bo = al(4 * (na + nb)), wsb = al(workspace_bytes_for(logn));
+    const uint64_t need = ba + bb + bo + 256 + wsb;
+    if (!budget_reserve(c, need)) {
+        set_error("HBM budget exhausted");
+        return B2M_ERR_OUT_OF_MEMORY;
+    }
+    void* mem = nullptr;
+    cudaError_t e = cudaMallocAsync(&mem, need, s);
+    if (e != cudaSuccess) {
+        budget_release(c, need);
+        return cuda_status(e, "cudaMallocAsync(autotune)");
+    }
+    unsigned char* base = static_cast<unsigned char*>(mem);
+    u32* da = reinterpret_cast<u32*>(base);
+    u32* db = reinterpret_cast<u32*>(base + ba);
+    u32* dout = reinterpret_cast<u32*>(base + ba + bb);
+    uint64_t* dlen = reinterpret_cast<uint64_t*>(base + ba + bb + bo);
+    void* ws = base + ba + bb + bo + 256;
+    e = launch_gen_operand(s, 12345, na, 0, da);
+    if (e == cudaSuccess) e = launch_gen_operand(s, 67890, nb, 0, db);
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreate(&t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&t1);
+    float best = 1e30f;
+    size_t best_i = 0;
+    uint32_t cnt = 0;
+    for (size_t i = 0; i < cands.size() && e == cudaSuccess; ++i) {
+        // one warm-up, then the median of three timed products
+        float ms[3];
+        for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+            e = cudaEventRecord(t0, s);
+            if (e == cudaSuccess) e = launch_product(da, na, db, nb, dout, dlen, ws, cands[i], c->tw, c->d_err, s);
+            if (e == cudaSuccess) e = cudaEventRecord(t1, s);
+            if (e == cudaSuccess) e = cudaEventSynchronize(t1);
+            if (e == cudaSuccess && rep > 0) cudaEventElapsedTime(&ms[rep - 1], t0, t1);
+        }
+        if (e != cudaSuccess) break;
+        std::sort(ms, ms + 3);
+        if (ms[1] < best) {
+            best = ms[1];
+            best_i = i;
+        }
+        if (cnt < cap) {
+            b2m_tune_entry& o = out[cnt++];
+            const Plan& p = cands[i];
+            o.plan.ntt_log2 = (uint32_t)logn;
+            o.plan.npass = (uint32_t)p.npass;
+            for (int k = 0; k < 3; ++k) {
+                o.plan.logr[k] = (uint32_t)p.logr[k];
+                o.plan.logc[k] = (uint32_t)p.logc[k];
+            }
+            o.plan.launches = (uint32_t)plan_launches(p);
+            o.ms = ms[1];
+            o.chosen = 0;
+        }
+    }
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    cudaFreeAsync(mem, s);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    budget_release(c, need);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return cuda_status(e, "autotune");
+    st = take_device_error(c);
+    if (st != B2M_OK) return st;
+    set_tuned(c, logn, cands[best_i]);
+    if (best_i < cnt) out[best_i].chosen = 1;
+    if (n) *n = cnt;
     return B2M_OK;
 }
 
@@ -290,7 +395,7 @@ b2m_status b2m_mul_device_traced(const uint32_t* d_a, uint64_t na, const uint32_
     if (st != B2M_OK) return st;
     cudaSetDevice(c->device);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const Plan p = make_plan(logn);
+    const Plan p = plan_for(c, logn);
     const uint64_t wsb = workspace_bytes_for(logn);
     if (!budget_reserve(c, wsb)) {
         set_error("HBM budget exhausted");
@@ -348,7 +453,7 @@ b2m_status b2m_mul_host(const uint32_t* a, uint64_t na, const uint32_t* b, uint6
     if (st != B2M_OK) return st;
     std::lock_guard<std::mutex> lk(c->host_mu);
     cudaSetDevice(c->device);
-    const Plan p = make_plan(logn);
+    const Plan p = plan_for(c, logn);
     auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
     const uint64_t ba = al(4 * na), bb = al(4 * nb), bo = al(4 * (na + nb)), bl = 256;
     const uint64_t wsb = workspace_bytes_for(logn);

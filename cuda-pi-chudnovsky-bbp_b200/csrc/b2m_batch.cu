@@ -94,9 +94,12 @@ static void free_batch(b2m_batch* bt) {
 // Time every candidate plan of bucket b on its own jobs; keep the fastest.
 static cudaError_t autotune_bucket(b2m_batch* bt, Bucket& b, cudaStream_t s) {
     Context* c = bt->ctx;
-    if (c->tuned_r0[b.logn] > 0) {
-        b.plan = make_plan_custom(b.logn, c->tuned_r0[b.logn], c->tuned_tile[b.logn]);
-        return cudaSuccess;
+    {
+        std::lock_guard<std::mutex> lk(c->tune_mu);
+        if (c->has_tuned[b.logn]) {
+            b.plan = c->tuned[b.logn];
+            return cudaSuccess;
+        }
     }
     std::vector<Plan> cands = plan_candidates(b.logn);
     if (cands.size() < 2) return cudaSuccess;
@@ -128,9 +131,7 @@ static cudaError_t autotune_bucket(b2m_batch* bt, Bucket& b, cudaStream_t s) {
     cudaEventDestroy(t1);
     if (e != cudaSuccess) return e;
     b.plan = best_p;
-    c->tuned_r0[b.logn] = best_p.logr[0];
-    // recover the tile exponent from the first pass geometry
-    c->tuned_tile[b.logn] = best_p.logr[0] + best_p.logc[0];
+    set_tuned(c, b.logn, best_p);
     return cudaSuccess;
 }
 
@@ -214,7 +215,7 @@ b2m_status b2m_batch_create(const b2m_job* jobs, uint64_t njobs, uint32_t flags,
       for (size_t off = 0; off < it->second.size(); off += MAX_GRID_Y) {
         Bucket b;
         b.logn = it->first;
-        b.plan = make_plan(b.logn);
+        b.plan = plan_for(c, b.logn);
         b.first = (unsigned)hj.size();
         b.njobs = (unsigned)std::min<size_t>(MAX_GRID_Y, it->second.size() - off);
         for (size_t k = off; k < off + b.njobs; ++k) {

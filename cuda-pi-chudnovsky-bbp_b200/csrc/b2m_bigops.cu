@@ -301,8 +301,7 @@ DV mul(Scope& S, DV a, DV b) {
     const b2m_status st = check_sizes(a.n, b.n, &logn);
     if (st != B2M_OK) throw Err{st};
     Context* c = S.c();
-    const Plan p = c->tuned_r0[logn] > 0 ? make_plan_custom(logn, c->tuned_r0[logn], c->tuned_tile[logn])
-                                         : make_plan(logn);
+    const Plan p = plan_for(c, logn);
     DV out = S.vec(a.n + b.n);
     void* ws = p.npass ? S.raw(workspace_bytes_for(logn)) : nullptr;
     uint64_t* d_len = reinterpret_cast<uint64_t*>(S.word() + 2);
@@ -587,8 +586,7 @@ void batched_mul(Scope& S, const u32* a, uint64_t sa, uint64_t na, const u32* b,
     const b2m_status st = check_sizes(na, nb, &logn);
     if (st != B2M_OK) throw Err{st};
     Context* c = S.c();
-    const Plan p = c->tuned_r0[logn] > 0 ? make_plan_custom(logn, c->tuned_r0[logn], c->tuned_tile[logn])
-                                         : make_plan(logn);
+    const Plan p = plan_for(c, logn);
     const uint64_t wss = p.npass ? ((workspace_bytes_for(logn) + 255) & ~255ull) : 0;
     // at most 65535 jobs a launch, and at most ~1 GiB of transform workspace
     uint64_t chunk = 65535;

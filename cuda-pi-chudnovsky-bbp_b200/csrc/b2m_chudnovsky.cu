@@ -470,8 +470,7 @@ static cudaError_t merge_level(Context* c, const LevelView& L, const uint64_t mx
         if ((school_mask >> k) & 1) continue;
         const int logn = ceil_log2(2 * cap[k]);
         if (logn > MAX_LOGN) return cudaErrorInvalidValue;
-        const Plan p = c->tuned_r0[logn] > 0 ? make_plan_custom(logn, c->tuned_r0[logn], c->tuned_tile[logn])
-                                             : make_plan(logn);
+        const Plan p = plan_for(c, logn);
         const uint64_t wss = logn > SMALL_MAX_LOGN ? al(workspace_bytes_for(logn)) : 0;
         const uint64_t tb = al(m2 * sizeof(ProdJob)) + m2 * wss;
         void* t = nullptr;

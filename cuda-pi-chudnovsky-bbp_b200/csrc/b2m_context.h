@@ -25,13 +25,26 @@ struct Context {
     std::mutex host_mu;                  // serialises b2m_mul_host (shared buffers)
     void* host_dev = nullptr;            // device buffers of b2m_mul_host, grown on demand
     uint64_t host_dev_cap = 0;
-    // Autotuned plans of batched buckets per transform length (-1: default).
-    int tuned_r0[MAX_LOGN + 1];
-    int tuned_tile[MAX_LOGN + 1];
+    // Autotuned plan per transform length (b2m_autotune, batch autotune);
+    // used by every product of that length once set.
+    std::mutex tune_mu;
+    Plan tuned[MAX_LOGN + 1];
+    bool has_tuned[MAX_LOGN + 1];
     Context() {
-        for (int i = 0; i <= MAX_LOGN; ++i) tuned_r0[i] = tuned_tile[i] = -1;
+        for (int i = 0; i <= MAX_LOGN; ++i) has_tuned[i] = false;
     }
 };
+
+// The plan products of transform length 2^logn use: the tuned one if any.
+inline Plan plan_for(Context* c, int logn) {
+    std::lock_guard<std::mutex> lk(c->tune_mu);
+    return c->has_tuned[logn] ? c->tuned[logn] : make_plan(logn);
+}
+inline void set_tuned(Context* c, int logn, const Plan& p) {
+    std::lock_guard<std::mutex> lk(c->tune_mu);
+    c->tuned[logn] = p;
+    c->has_tuned[logn] = true;
+}
 
 extern Context* g_ctx;
 extern std::mutex g_ctx_mu;

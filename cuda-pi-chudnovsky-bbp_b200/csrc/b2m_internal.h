@@ -38,6 +38,7 @@ struct Plan {
 
 Plan make_plan(int logn);
 Plan make_plan_custom(int logn, int r0, int tile);
+Plan make_plan_split(int logn, const int* r, int npass, int tile);
 std::vector<Plan> plan_candidates(int logn);
 
 // Per-product workspace layout (bytes): two N-element u64 arrays plus the

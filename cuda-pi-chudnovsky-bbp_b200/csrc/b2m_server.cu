@@ -216,7 +216,7 @@ static cudaError_t launch_dispatch(b2m_server* S, Slot& sl, std::vector<Req>& rv
         const int logn = rs[order[k0]]->logn;
         size_t k1 = k0;
         while (k1 < n && rs[order[k1]]->logn == logn && k1 - k0 < 65535) ++k1;
-        const Plan p = make_plan(logn);
+        const Plan p = plan_for(S->c, logn);
         if ((e = launch_bucket(p, djobs + k0, (unsigned)(k1 - k0), S->c->tw, S->c->d_err, s)) != cudaSuccess) return e;
         k0 = k1;
     }

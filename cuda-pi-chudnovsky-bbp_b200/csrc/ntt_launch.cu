@@ -17,6 +17,8 @@
 
 #include <vector>
 
+#include <algorithm>
+
 #include "b2m.h"
 #include "b2m_internal.h"
 #include "carry.cuh"
@@ -29,40 +31,49 @@ Plan make_plan(int logn) { return make_plan_custom(logn, -1, -1); }
 // keeping at least 4 columns (32-byte rows) in a 2^14-element tile and the
 // last (contiguous) pass taking up to 2^14; three passes above.
 Plan make_plan_custom(int logn, int r0, int tile) {
+    if (logn <= SMALL_MAX_LOGN) return make_plan_split(logn, nullptr, 0, tile);
+    int r[3];
+    if (logn <= 26) {
+        r[0] = r0 > 0 ? r0 : (logn / 2 < 12 ? logn / 2 : 12);
+        r[1] = logn - r[0];
+        return make_plan_split(logn, r, 2, tile);
+    }
+    r[0] = logn / 3;
+    r[1] = logn / 3;
+    r[2] = logn - 2 * (logn / 3);
+    return make_plan_split(logn, r, 3, tile);
+}
+
+// Explicit pass radices r[0..npass) (sum logn) with one tile size (log2
+// elements, <= 0 for the default); npass = 0 is the single-CTA product.
+Plan make_plan_split(int logn, const int* r, int npass, int tile) {
     Plan p;
     p.logn = logn;
-    if (logn <= SMALL_MAX_LOGN) {
-        p.npass = 0;
-        return p;
-    }
-    if (logn <= 26) {
-        p.npass = 2;
-        p.logr[0] = r0 > 0 ? r0 : (logn / 2 < 12 ? logn / 2 : 12);
-        p.logr[1] = logn - p.logr[0];
-    } else {
-        p.npass = 3;
-        p.logr[0] = logn / 3;
-        p.logr[1] = logn / 3;
-        p.logr[2] = logn - 2 * (logn / 3);
-    }
+    p.npass = npass;
+    if (npass == 0) return p;
+    for (int k = 0; k < npass; ++k) p.logr[k] = r[k];
     if (tile <= 0) tile = logn >= 20 ? 14 : (logn >= 17 ? 13 : 12);
     int before = 0;
     for (int k = 0; k < p.npass; ++k) {
-        const int r = p.logr[k];
-        const int after = logn - before - r;  // log2 S
-        int c = tile - r;
+        const int rk = p.logr[k];
+        const int after = logn - before - rk;  // log2 S
+        int c = tile - rk;
         if (c < 0) c = 0;
-        const int cap = (k + 1 < p.npass) ? after : (logn - r);
+        const int cap = (k + 1 < p.npass) ? after : (logn - rk);
         if (c > cap) c = cap;
         p.logc[k] = c;
-        before += r;
+        before += rk;
     }
     return p;
 }
 
+// Plans the autotuners time: every two-pass split with a first radix of
+// 2^7..2^12 and a last of 2^7..2^14, and the balanced three-pass splits (each
+// radix within one of logn / 3), each at tiles of 2^12, 2^13 and 2^14
+// elements where the radices fit.
 std::vector<Plan> plan_candidates(int logn) {
     std::vector<Plan> v;
-    if (logn <= SMALL_MAX_LOGN || logn > 26) {
+    if (logn <= SMALL_MAX_LOGN) {
         v.push_back(make_plan(logn));
         return v;
     }
@@ -70,10 +81,25 @@ std::vector<Plan> plan_candidates(int logn) {
         const int r1 = logn - r0;
         if (r1 < 7 || r1 > 14) continue;
         for (int tile = 12; tile <= 14; ++tile) {
-            if (r1 > tile && tile < 14) continue;  // last pass needs its whole column in the tile
-            v.push_back(make_plan_custom(logn, r0, tile));
+            if (r0 > tile || r1 > tile) continue;
+            const int r[2] = {r0, r1};
+            v.push_back(make_plan_split(logn, r, 2, tile));
         }
     }
+    if (logn >= 21) {
+        const int t = logn / 3;
+        for (int r0 = std::max(7, t - 1); r0 <= std::min(12, t + 1); ++r0)
+            for (int r1 = std::max(7, t - 1); r1 <= std::min(12, t + 1); ++r1) {
+                const int r2 = logn - r0 - r1;
+                if (r2 < 7 || r2 > 14) continue;
+                for (int tile = 12; tile <= 14; ++tile) {
+                    if (r0 > tile || r1 > tile || r2 > tile) continue;
+                    const int r[3] = {r0, r1, r2};
+                    v.push_back(make_plan_split(logn, r, 3, tile));
+                }
+            }
+    }
+    if (v.empty()) v.push_back(make_plan(logn));
     return v;
 }
 

@@ -345,6 +345,27 @@ typedef struct b2m_plan_desc {
  * reference counterpart: the reference always runs radix-2 stages). */
 b2m_status b2m_plan_describe(uint64_t na, uint64_t nb, b2m_plan_desc* desc);
 
+/* One timed candidate of b2m_autotune. */
+typedef struct b2m_tune_entry {
+    b2m_plan_desc plan;
+    float ms;               /* median device time of one product with that plan */
+    uint32_t chosen;        /* 1 for the plan that was kept */
+} b2m_tune_entry;
+
+/* No reference counterpart. Times every candidate transform plan (pass
+ * splits and tile sizes) for an na x nb product on `stream`, with seeded
+ * operands in a temporary allocation, and keeps the fastest: every later
+ * product of the same transform length (single, batched, tree, division,
+ * serving) uses it. Synchronous. Up to cap timings go to out (may be NULL
+ * with cap 0), *n receives how many were written. */
+b2m_status b2m_autotune(uint64_t na, uint64_t nb, b2m_stream stream, b2m_tune_entry* out, uint32_t cap,
+                        uint32_t* n);
+
+/* Fixes the plan of one transform length (desc->ntt_log2) to desc, which
+ * must be one of the candidates b2m_autotune times (its out entries are
+ * valid input). For reproducible timings and for testing every plan. */
+b2m_status b2m_set_plan(const b2m_plan_desc* desc);
+
 typedef struct b2m_kernel_time {
     uint32_t kind;          /* B2M_K_* */
     uint32_t logr;          /* pass radix exponent (0 for carry) */
