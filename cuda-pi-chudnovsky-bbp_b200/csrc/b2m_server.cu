@@ -13,8 +13,10 @@
 // Every product is checked on the device modulo 2^32 - 1 and 2^32 + 1 (limb
 // sums and alternating sums of operands and product) before it is reported
 // done; workspace returns to the budget at completion, owned buffers at
-// b2m_server_release. The scheduler never waits on the device: it polls
-// completion events.
+// b2m_server_release. Each slot keeps its dispatch blocks (job tables and
+// transform workspaces) in one device arena that only grows, so steady-state
+// dispatches allocate nothing large. The scheduler never waits on the device:
+// it polls completion events.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -109,6 +111,11 @@ struct Slot {
     std::vector<uint64_t> ids;
     void* block = nullptr;        // dispatch block: job table, lengths, residues, workspaces
     uint64_t block_bytes = 0;
+    // The slot's dispatch blocks live in one arena that only grows: a slot
+    // runs one dispatch at a time, and a fresh multi-GB stream-ordered
+    // allocation per dispatch cost the scheduler thread ~80 ms of mapping.
+    void* arena = nullptr;
+    uint64_t arena_cap = 0;
     void* host = nullptr;         // pinned: lengths + residues + error word
     uint64_t host_cap = 0;
 };
@@ -165,7 +172,25 @@ static cudaError_t launch_dispatch(b2m_server* S, Slot& sl, std::vector<Req>& rv
             scr += al(carry_scratch_bytes(q->logn));
         }
     sl.block_bytes = tab + lens + res + bufs + scr;
-    if ((e = cudaMallocAsync(&sl.block, sl.block_bytes, s)) != cudaSuccess) return e;
+    if (sl.block_bytes > sl.arena_cap) {
+        // grow by at least a quarter, in 256 MiB steps (the previous dispatch
+        // on this slot has completed, so its arena can go)
+        const uint64_t cap = al(std::max<uint64_t>(sl.block_bytes, sl.arena_cap + sl.arena_cap / 4) + (256ull << 20)) &
+                             ~((256ull << 20) - 1);
+        if (sl.arena) {
+            cudaFreeAsync(sl.arena, s);
+            budget_release(S->c, sl.arena_cap);
+            sl.arena = nullptr;
+            sl.arena_cap = 0;
+        }
+        if (!budget_reserve(S->c, cap)) return cudaErrorMemoryAllocation;
+        if ((e = cudaMallocAsync(&sl.arena, cap, s)) != cudaSuccess) {
+            budget_release(S->c, cap);
+            return e;
+        }
+        sl.arena_cap = cap;
+    }
+    sl.block = sl.arena;
     unsigned char* base = static_cast<unsigned char*>(sl.block);
     ProdJob* djobs = reinterpret_cast<ProdJob*>(base);
     u64* dlens = reinterpret_cast<u64*>(base + tab);
@@ -218,23 +243,21 @@ static cudaError_t launch_dispatch(b2m_server* S, Slot& sl, std::vector<Req>& rv
         while (k1 < n && rs[order[k1]]->logn == logn && k1 - k0 < 65535) ++k1;
         const Plan p = plan_for(S->c, logn);
         if ((e = launch_bucket(p, djobs + k0, (unsigned)(k1 - k0), S->c->tw, S->c->d_err, s)) != cudaSuccess) return e;
+        // Residue check of the bucket's products, its grid sized to the
+        // bucket's longest operands (not the dispatch's).
+        uint64_t maxlen = 0;
+        for (size_t k = k0; k < k1; ++k) maxlen = std::max<uint64_t>(maxlen, rs[order[k]]->r.na + rs[order[k]]->r.nb);
+        const unsigned gx = (unsigned)((maxlen + 4095) / 4096);
+        k_residues<<<dim3(gx, (unsigned)(k1 - k0)), 256, 0, s>>>(djobs + k0, dres + k0 * RES_WORDS);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
         k0 = k1;
     }
-    // Residue check of every product, then results to pinned host memory.
-    uint64_t maxlen = 0;
-    for (Req* q : rs) maxlen = std::max<uint64_t>(maxlen, q->r.na + q->r.nb);
-    const unsigned gx = (unsigned)((maxlen + 4095) / 4096);
-    for (size_t k0 = 0; k0 < n; k0 += 65535) {
-        const unsigned ny = (unsigned)std::min<size_t>(65535, n - k0);
-        k_residues<<<dim3(gx, ny), 256, 0, s>>>(djobs + k0, dres + k0 * RES_WORDS);
-    }
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // Results to pinned host memory.
     unsigned char* h = static_cast<unsigned char*>(sl.host);
     if ((e = cudaMemcpyAsync(h, dlens, n * 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
     if ((e = cudaMemcpyAsync(h + lens, dres, n * RES_WORDS * 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
     if ((e = cudaMemcpyAsync(h + lens + res, S->c->d_err, 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
-    if ((e = cudaFreeAsync(sl.block, s)) != cudaSuccess) return e;
-    sl.block = nullptr;
+    sl.block = nullptr;  // the arena stays with the slot
     return cudaEventRecord(sl.ev, s);
 }
 
@@ -257,8 +280,7 @@ static void scheduler(b2m_server* S) {
             std::lock_guard<std::mutex> lk(S->mu);
             for (size_t k = 0; k < n; ++k) {
                 Req& r = S->reqs[sl.ids[k]];
-                S->used -= r.ws_bytes;
-                budget_release(S->c, r.ws_bytes);
+                S->used -= r.ws_bytes;  // the slot's arena holds the device memory itself
                 r.ws_bytes = 0;
                 r.t_done = t;
                 if (q != cudaSuccess) {
@@ -291,7 +313,7 @@ static void scheduler(b2m_server* S) {
                     Req& r = S->reqs[S->pending.front()];
                     const uint64_t need = r.own_bytes + r.ws_bytes;
                     if (S->used + need > S->cfg.hbm_budget_bytes) break;  // FIFO: wait for memory
-                    if (!budget_reserve(S->c, need)) break;
+                    if (!budget_reserve(S->c, r.own_bytes)) break;  // workspace: reserved by the arenas
                     S->used += need;
                     S->st.peak_bytes = std::max<uint64_t>(S->st.peak_bytes, S->used);
                     r.state = 1;
@@ -317,7 +339,6 @@ static void scheduler(b2m_server* S) {
                     r.status = e == cudaErrorMemoryAllocation ? B2M_ERR_OUT_OF_MEMORY : B2M_ERR_CUDA;
                     r.t_done = now_ns();
                     S->used -= r.ws_bytes;
-                    budget_release(S->c, r.ws_bytes);
                     r.ws_bytes = 0;
                     ++S->st.failed;
                 }
@@ -504,6 +525,10 @@ b2m_status b2m_server_stop(b2m_server* S) {
     cudaStreamSynchronize(S->release_stream);
     for (Slot& sl : S->slots) {
         cudaStreamSynchronize(sl.s);
+        if (sl.arena) {
+            cudaFree(sl.arena);
+            budget_release(S->c, sl.arena_cap);
+        }
         if (sl.host) cudaFreeHost(sl.host);
         cudaEventDestroy(sl.ev);
         cudaStreamDestroy(sl.s);
