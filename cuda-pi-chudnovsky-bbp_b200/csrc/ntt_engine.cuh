@@ -185,6 +185,34 @@ __device__ __forceinline__ void lead_step(u64* sm, const u64* __restrict__ dtw) 
     });
 }
 
+// Level-1 twiddles of a radix-64 group, slot i (k1 = brev3(i)) times
+// 8^(u1 * k1) = 2^(3 u1 k1) (inverse: its inverse), with u1 a compile-time
+// constant so every shift folds to its fixed word offset.
+template <int U1, bool INV>
+__device__ __forceinline__ void level1_twiddle(u64* x) {
+#pragma unroll
+    for (int i = 1; i < 8; ++i) {
+        const int s = 3 * U1 * brev_c(i, 3);
+        x[i] = gl_shl(x[i], INV ? (s ? 192 - s : 0) : s);
+    }
+}
+
+// The same for a warp-uniform run-time u1 in [0, 8): one uniform branch to
+// the compile-time form.
+template <bool INV>
+__device__ __forceinline__ void level1_twiddle(u64* x, int u1) {
+    switch (u1) {
+        case 0: break;
+        case 1: level1_twiddle<1, INV>(x); break;
+        case 2: level1_twiddle<2, INV>(x); break;
+        case 3: level1_twiddle<3, INV>(x); break;
+        case 4: level1_twiddle<4, INV>(x); break;
+        case 5: level1_twiddle<5, INV>(x); break;
+        case 6: level1_twiddle<6, INV>(x); break;
+        default: level1_twiddle<7, INV>(x); break;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Radix-64 group on blocks of L = 2^LOGL rows: instance (col, blk, j) with
 // j in [0, L/64) owns rows blk*L + j + u*(L/64), u in [0, 64), u = u1 + 8*u2.
@@ -214,14 +242,9 @@ __device__ __forceinline__ void group64(u64* sm, const u64* __restrict__ dtw) {
             for (int m = 0; m < 8; ++m) x[m] = ptr[m * st];
             if (!INV) {
                 dft_fwd<8>(x);
-#pragma unroll
-                for (int i = 1; i < 8; ++i) x[i] = gl_shl(x[i], 3 * u1 * brev_c(i, 3));
+                level1_twiddle<false>(x, u1);
             } else {
-#pragma unroll
-                for (int i = 1; i < 8; ++i) {
-                    const int s = 3 * u1 * brev_c(i, 3);
-                    x[i] = gl_shl(x[i], s ? 192 - s : 0);
-                }
+                level1_twiddle<true>(x, u1);
                 dft_inv<8>(x);
             }
 #pragma unroll
