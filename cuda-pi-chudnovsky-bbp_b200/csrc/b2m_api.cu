@@ -80,6 +80,7 @@ static void destroy_context(Context* c) {
     if (c->hstream) cudaStreamSynchronize(c->hstream);
     if (c->hcopy) cudaStreamSynchronize(c->hcopy);
     if (c->host_dev) cudaFree(c->host_dev);
+    twtable_free_all(c);
     if (c->d_tables) cudaFree(c->d_tables);
     if (c->d_err) cudaFree(c->d_err);
     if (c->hstream) cudaStreamDestroy(c->hstream);
@@ -246,6 +247,7 @@ b2m_status b2m_mul_device(const uint32_t* d_a, uint64_t na, const uint32_t* d_b,
     if (st != B2M_OK) return st;
     cudaSetDevice(c->device);
     const Plan p = plan_for(c, logn);
+    if (cudaError_t te = twtable_ensure(c, p, s)) return cuda_status(te, "twiddle table");
     const uint64_t wsb = workspace_bytes_for(logn);
     if (!budget_reserve(c, wsb)) {
         set_error("HBM budget exhausted");
@@ -341,6 +343,7 @@ b2m_status b2m_autotune(uint64_t na, uint64_t nb, b2m_stream stream, b2m_tune_en
     for (size_t i = 0; i < cands.size() && e == cudaSuccess; ++i) {
         // one warm-up, then the median of three timed products
         float ms[3];
+        e = twtable_ensure(c, cands[i], s);
         for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
             e = cudaEventRecord(t0, s);
             if (e == cudaSuccess) e = launch_product(da, na, db, nb, dout, dlen, ws, cands[i], c->tw, c->d_err, s);
@@ -396,6 +399,7 @@ b2m_status b2m_mul_device_traced(const uint32_t* d_a, uint64_t na, const uint32_
     cudaSetDevice(c->device);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const Plan p = plan_for(c, logn);
+    if (cudaError_t te = twtable_ensure(c, p, s)) return cuda_status(te, "twiddle table");
     const uint64_t wsb = workspace_bytes_for(logn);
     if (!budget_reserve(c, wsb)) {
         set_error("HBM budget exhausted");
@@ -485,6 +489,7 @@ b2m_status b2m_mul_host(const uint32_t* a, uint64_t na, const uint32_t* b, uint6
     void* ws = base + ba + bb + bo + bl;
     cudaStream_t s = c->hstream;
     cudaError_t e;
+    if ((e = twtable_ensure(c, p, s)) != cudaSuccess) return cuda_status(e, "twiddle table");
     // Operand B crosses the bus after A, on a second stream, while A's forward
     // transform runs: the product waits for B only before B's transform.
     if ((e = cudaMemcpyAsync(da, a, 4 * na, cudaMemcpyHostToDevice, s)) != cudaSuccess ||

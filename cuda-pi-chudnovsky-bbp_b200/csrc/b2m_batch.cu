@@ -111,6 +111,7 @@ static cudaError_t autotune_bucket(b2m_batch* bt, Bucket& b, cudaStream_t s) {
     cudaError_t e = cudaSuccess;
     for (const Plan& p : cands) {
         float ms_sum = 0;
+        if ((e = twtable_ensure(c, p, s)) != cudaSuccess) break;
         for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
             launch_batch_prep(s, bt->djobs, bt->njobs_all, bt->scratch, bt->scratch_words);
             cudaEventRecord(t0, s);
@@ -252,6 +253,11 @@ b2m_status b2m_batch_create(const b2m_job* jobs, uint64_t njobs, uint32_t flags,
                 return cuda_status(e, "autotune");
             }
     }
+    for (Bucket& b : bt->buckets)  // twiddle tables exist before any capture
+        if ((e = twtable_ensure(c, b.plan, bt->side[0])) != cudaSuccess) {
+            free_batch(bt);
+            return cuda_status(e, "twiddle table");
+        }
     if (flags & B2M_BATCH_GRAPH) {
         cudaStream_t cs;
         cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);

@@ -302,6 +302,7 @@ DV mul(Scope& S, DV a, DV b) {
     if (st != B2M_OK) throw Err{st};
     Context* c = S.c();
     const Plan p = plan_for(c, logn);
+    ck(twtable_ensure(c, p, S.s()), "twiddle table");
     DV out = S.vec(a.n + b.n);
     void* ws = p.npass ? S.raw(workspace_bytes_for(logn)) : nullptr;
     uint64_t* d_len = reinterpret_cast<uint64_t*>(S.word() + 2);
@@ -587,6 +588,7 @@ void batched_mul(Scope& S, const u32* a, uint64_t sa, uint64_t na, const u32* b,
     if (st != B2M_OK) throw Err{st};
     Context* c = S.c();
     const Plan p = plan_for(c, logn);
+    ck(twtable_ensure(c, p, S.s()), "twiddle table");
     const uint64_t wss = p.npass ? ((workspace_bytes_for(logn) + 255) & ~255ull) : 0;
     // at most 65535 jobs a launch, and at most ~1 GiB of transform workspace
     uint64_t chunk = 65535;

@@ -471,6 +471,7 @@ static cudaError_t merge_level(Context* c, const LevelView& L, const uint64_t mx
         const int logn = ceil_log2(2 * cap[k]);
         if (logn > MAX_LOGN) return cudaErrorInvalidValue;
         const Plan p = plan_for(c, logn);
+        if ((e = twtable_ensure(c, p, s)) != cudaSuccess) break;
         const uint64_t wss = logn > SMALL_MAX_LOGN ? al(workspace_bytes_for(logn)) : 0;
         const uint64_t tb = al(m2 * sizeof(ProdJob)) + m2 * wss;
         void* t = nullptr;

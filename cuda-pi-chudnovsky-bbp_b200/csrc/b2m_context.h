@@ -5,6 +5,7 @@
 #include <atomic>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "b2m.h"
 #include "b2m_internal.h"
@@ -25,6 +26,15 @@ struct Context {
     std::mutex host_mu;                  // serialises b2m_mul_host (shared buffers)
     void* host_dev = nullptr;            // device buffers of b2m_mul_host, grown on demand
     uint64_t host_dev_cap = 0;
+    // Inter-pass twiddle tables (twtable_ensure), keyed by (logm, logr).
+    struct TwTable {
+        int logm, logr;
+        u64* fwd;
+        u64* inv;
+        uint64_t bytes;
+    };
+    std::mutex twt_mu;
+    std::vector<TwTable> twt;
     // Autotuned plan per transform length (b2m_autotune, batch autotune);
     // used by every product of that length once set.
     std::mutex tune_mu;

@@ -112,8 +112,23 @@ struct PassGeo {
     int logr = 0, logc = 0, logs = 0, logm = 0;
     unsigned grid = 0, block = 0;
     size_t smem = 0;
+    // Inter-pass twiddles of this pass in data order (w_M^(bitrev(row) * c)
+    // at (row << logs) + c), forward and inverse, when a table exists for
+    // (logm, logr); null: the kernels build each twiddle from u1 * u2.
+    const u64* tfwd = nullptr;
+    const u64* tinv = nullptr;
 };
 PassGeo pass_geo(const Plan& p, int k);
+
+// Inter-pass twiddle tables, per (logm, logr), kept for the context's life.
+// twtable_ensure builds the ones plan p needs (only for M >= 2^TWT_MIN_LOGM,
+// never while `s` is capturing, skipped if the budget is short); pass_geo
+// only looks them up, so launch paths that must not allocate still use
+// tables that exist.
+constexpr int TWT_MIN_LOGM = 20;
+struct Context;
+cudaError_t twtable_ensure(Context* c, const Plan& p, cudaStream_t s);
+void twtable_free_all(Context* c);
 
 // Per-family launchers (ntt_fam_*.cu, ntt_carry.cu); each dispatches on the
 // radix exponent to the matching template instantiation.

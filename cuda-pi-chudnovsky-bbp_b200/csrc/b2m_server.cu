@@ -242,6 +242,7 @@ static cudaError_t launch_dispatch(b2m_server* S, Slot& sl, std::vector<Req>& rv
         size_t k1 = k0;
         while (k1 < n && rs[order[k1]]->logn == logn && k1 - k0 < 65535) ++k1;
         const Plan p = plan_for(S->c, logn);
+        if ((e = twtable_ensure(S->c, p, s)) != cudaSuccess) return e;
         if ((e = launch_bucket(p, djobs + k0, (unsigned)(k1 - k0), S->c->tw, S->c->d_err, s)) != cudaSuccess) return e;
         // Residue check of the bucket's products, its grid sized to the
         // bucket's longest operands (not the dispatch's).

@@ -28,17 +28,17 @@ FAMILIES = [
         ("k_fwd_first", COL, "launch_fwd_first",
          "(int logr, const PassGeo& g, cudaStream_t s, const u32* limbs, u64 ndig, u64* out, "
          "const RootTables& tw, const ProdJob* jobs, unsigned njobs, int operand)",
-         "(limbs, ndig, out, g.logs, g.logm, tw, jobs, operand)", "dim3(g.grid, njobs)")]),
+         "(limbs, ndig, out, g.logs, g.logm, tw, g.tfwd, jobs, operand)", "dim3(g.grid, njobs)")]),
     ("ntt_fam_mid.cu", "middle forward passes", "mid", [
         ("k_fwd_mid", COL, "launch_fwd_mid",
          "(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw, const ProdJob* jobs, "
          "unsigned njobs, int operand)",
-         "(buf, g.logs, g.logm, tw, jobs, operand)", "dim3(g.grid, njobs)")]),
+         "(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand)", "dim3(g.grid, njobs)")]),
     ("ntt_fam_inv.cu", "non-last inverse passes", "inv", [
         ("k_inv_mid", COL, "launch_inv_mid",
          "(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw, const ProdJob* jobs, "
          "unsigned njobs)",
-         "(buf, g.logs, g.logm, tw, jobs)", "dim3(g.grid, njobs)")]),
+         "(buf, g.logs, g.logm, tw, g.tinv, jobs)", "dim3(g.grid, njobs)")]),
     ("ntt_fam_last.cu", "last forward pass of operand A", "last", [
         ("k_fwd_last", ROW, "launch_fwd_last",
          "(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw, const ProdJob* jobs, "

@@ -54,7 +54,7 @@ struct ColPass {
     static constexpr int PER = (TL::R * TL::C) / TL::T;
     static_assert(PER == 16 && DR >= 1, "16 elements per thread");
     int col, row0, sa0;
-    u64 gi0, gstep;
+    u64 gi0, gstep, ti0;  // ti0: index in the pass's twiddle table (row0, c)
     u32 e0, ec;
     __device__ __forceinline__ ColPass(int logS, int logM) {
         col = (int)threadIdx.x & (TL::C - 1);
@@ -63,6 +63,7 @@ struct ColPass {
         const u64 g = ((u64)blockIdx.x << TL::LC) + col;
         const u64 c = g & ((1ull << logS) - 1);
         gi0 = ((g >> logS) << (TL::LR + logS)) + ((u64)row0 << logS) + c;
+        ti0 = ((u64)row0 << logS) + c;
         gstep = (u64)DR << logS;
         const u32 sh = 32 - logM;
         const u32 f0 = __brev((u32)row0) >> (32 - TL::LR);
@@ -100,7 +101,7 @@ struct RowPass {
 template <int LOGR, int LOGC>
 __global__ void B2M_PASS_BOUNDS((Tile<LOGR, LOGC, MAP_COL>::T))
 k_fwd_first(const u32* __restrict__ limbs, u64 ndig, u64* __restrict__ out, int logS, int logM, RootTables tw,
-            const ProdJob* __restrict__ jobs, int operand) {
+            const u64* __restrict__ ttab, const ProdJob* __restrict__ jobs, int operand) {
     using TL = Tile<LOGR, LOGC, MAP_COL>;
     using G = ColPass<TL>;
     extern __shared__ u64 sm[];
@@ -115,19 +116,26 @@ k_fwd_first(const u32* __restrict__ limbs, u64 ndig, u64* __restrict__ out, int 
     for (int k = 0; k < G::PER; ++k) sm[gp.sa0 + G::soff(k)] = digit_of(limbs, ndig, gp.gi0 + k * gp.gstep);
     __syncthreads();
     tile_fwd<TL>(sm, tw.dtw);
+    if (ttab) {
 #pragma unroll
-    for (int k = 0; k < G::PER; ++k) {
-        u64 x = sm[gp.sa0 + G::soff(k)];
-        const u32 e = gp.e0 + G::fk(k) * gp.ec;
-        if (e) x = gl_mul(x, uroot(e, tw.u1, tw.u2));
-        out[gp.gi0 + k * gp.gstep] = x;
+        for (int k = 0; k < G::PER; ++k)
+            out[gp.gi0 + k * gp.gstep] = gl_mul(sm[gp.sa0 + G::soff(k)], __ldg(ttab + gp.ti0 + k * gp.gstep));
+    } else {
+#pragma unroll
+        for (int k = 0; k < G::PER; ++k) {
+            u64 x = sm[gp.sa0 + G::soff(k)];
+            const u32 e = gp.e0 + G::fk(k) * gp.ec;
+            if (e) x = gl_mul(x, uroot(e, tw.u1, tw.u2));
+            out[gp.gi0 + k * gp.gstep] = x;
+        }
     }
 }
 
 // A later, not-last forward pass, in place.
 template <int LOGR, int LOGC>
 __global__ void B2M_PASS_BOUNDS((Tile<LOGR, LOGC, MAP_COL>::T))
-k_fwd_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const ProdJob* __restrict__ jobs, int operand) {
+k_fwd_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const u64* __restrict__ ttab,
+          const ProdJob* __restrict__ jobs, int operand) {
     using TL = Tile<LOGR, LOGC, MAP_COL>;
     using G = ColPass<TL>;
     extern __shared__ u64 sm[];
@@ -137,12 +145,18 @@ k_fwd_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const ProdJo
     for (int k = 0; k < G::PER; ++k) sm[gp.sa0 + G::soff(k)] = buf[gp.gi0 + k * gp.gstep];
     __syncthreads();
     tile_fwd<TL>(sm, tw.dtw);
+    if (ttab) {
 #pragma unroll
-    for (int k = 0; k < G::PER; ++k) {
-        u64 x = sm[gp.sa0 + G::soff(k)];
-        const u32 e = gp.e0 + G::fk(k) * gp.ec;
-        if (e) x = gl_mul(x, uroot(e, tw.u1, tw.u2));
-        buf[gp.gi0 + k * gp.gstep] = x;
+        for (int k = 0; k < G::PER; ++k)
+            buf[gp.gi0 + k * gp.gstep] = gl_mul(sm[gp.sa0 + G::soff(k)], __ldg(ttab + gp.ti0 + k * gp.gstep));
+    } else {
+#pragma unroll
+        for (int k = 0; k < G::PER; ++k) {
+            u64 x = sm[gp.sa0 + G::soff(k)];
+            const u32 e = gp.e0 + G::fk(k) * gp.ec;
+            if (e) x = gl_mul(x, uroot(e, tw.u1, tw.u2));
+            buf[gp.gi0 + k * gp.gstep] = x;
+        }
     }
 }
 
@@ -151,18 +165,25 @@ k_fwd_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const ProdJo
 // coefficients (N^-1 already applied) in natural order.
 template <int LOGR, int LOGC>
 __global__ void B2M_PASS_BOUNDS((Tile<LOGR, LOGC, MAP_COL>::T))
-k_inv_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const ProdJob* __restrict__ jobs) {
+k_inv_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const u64* __restrict__ ttab,
+          const ProdJob* __restrict__ jobs) {
     using TL = Tile<LOGR, LOGC, MAP_COL>;
     using G = ColPass<TL>;
     extern __shared__ u64 sm[];
     if (jobs) buf = jobs[blockIdx.y].bufB;
     const G gp(logS, logM);
+    if (ttab) {
 #pragma unroll
-    for (int k = 0; k < G::PER; ++k) {
-        u64 x = buf[gp.gi0 + k * gp.gstep];
-        const u32 e = gp.e0 + G::fk(k) * gp.ec;
-        if (e) x = gl_mul(x, uroot(0u - e, tw.u1, tw.u2));
-        sm[gp.sa0 + G::soff(k)] = x;
+        for (int k = 0; k < G::PER; ++k)
+            sm[gp.sa0 + G::soff(k)] = gl_mul(buf[gp.gi0 + k * gp.gstep], __ldg(ttab + gp.ti0 + k * gp.gstep));
+    } else {
+#pragma unroll
+        for (int k = 0; k < G::PER; ++k) {
+            u64 x = buf[gp.gi0 + k * gp.gstep];
+            const u32 e = gp.e0 + G::fk(k) * gp.ec;
+            if (e) x = gl_mul(x, uroot(0u - e, tw.u1, tw.u2));
+            sm[gp.sa0 + G::soff(k)] = x;
+        }
     }
     __syncthreads();
     tile_inv<TL>(sm, tw.dtw);

@@ -20,8 +20,10 @@
 #include <algorithm>
 
 #include "b2m.h"
+#include "b2m_context.h"
 #include "b2m_internal.h"
 #include "carry.cuh"
+#include "ntt_engine.cuh"
 
 namespace b2m {
 
@@ -117,7 +119,74 @@ PassGeo pass_geo(const Plan& p, int k) {
     g.block = (unsigned)(1u << (logt < 10 ? logt : 10));
     const size_t rp = (size_t)(1 << g.logr) + (size_t)((1 << g.logr) >> 6);
     g.smem = rp * ((size_t)1 << g.logc) * sizeof(u64);
+    Context* c = ctx();
+    if (c && k + 1 < p.npass && g.logm >= TWT_MIN_LOGM) {
+        std::lock_guard<std::mutex> lk(c->twt_mu);
+        for (const Context::TwTable& t : c->twt)
+            if (t.logm == g.logm && t.logr == g.logr) {
+                g.tfwd = t.fwd;
+                g.tinv = t.inv;
+                break;
+            }
+    }
     return g;
+}
+
+// fwd[i] = w_M^(brev(row) * col), inv[i] = its inverse, i = (row << logs) + col:
+// the same exponent the pass kernels form (bitrev(row) * col * 2^(32 - logM)).
+__global__ void k_build_twtable(u64* __restrict__ fwd, u64* __restrict__ inv, int logm, int logr, RootTables tw) {
+    const int logs = logm - logr;
+    const u64 m = 1ull << logm;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (u64)gridDim.x * blockDim.x) {
+        const u32 row = (u32)(i >> logs), col = (u32)(i & ((1ull << logs) - 1));
+        const u64 f = __brev(row) >> (32 - logr);
+        const u32 e = (u32)((f * col) << (32 - logm));
+        fwd[i] = e ? uroot(e, tw.u1, tw.u2) : 1ull;
+        inv[i] = e ? uroot(0u - e, tw.u1, tw.u2) : 1ull;
+    }
+}
+
+cudaError_t twtable_ensure(Context* c, const Plan& p, cudaStream_t s) {
+    if (!c || p.npass < 2) return cudaSuccess;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return cudaSuccess;
+    for (int k = 0; k + 1 < p.npass; ++k) {
+        const PassGeo g = pass_geo(p, k);
+        if (g.logm < TWT_MIN_LOGM || g.tfwd) continue;
+        std::lock_guard<std::mutex> lk(c->twt_mu);
+        bool have = false;
+        for (const Context::TwTable& t : c->twt) have |= (t.logm == g.logm && t.logr == g.logr);
+        if (have) continue;
+        const uint64_t bytes = 2 * (8ull << g.logm);
+        if (!budget_reserve(c, bytes)) continue;  // no room: the kernels build twiddles instead
+        u64* mem = nullptr;
+        cudaError_t e = cudaMalloc(&mem, bytes);
+        if (e != cudaSuccess) {
+            budget_release(c, bytes);
+            cudaGetLastError();
+            continue;
+        }
+        const u64 m = 1ull << g.logm;
+        k_build_twtable<<<(unsigned)std::min<u64>(65535, (m + 255) / 256), 256, 0, s>>>(mem, mem + m, g.logm, g.logr,
+                                                                                      c->tw);
+        if ((e = cudaGetLastError()) == cudaSuccess) e = cudaStreamSynchronize(s);  // built before anyone sees it
+        if (e != cudaSuccess) {
+            cudaFree(mem);
+            budget_release(c, bytes);
+            return e;
+        }
+        c->twt.push_back({g.logm, g.logr, mem, mem + m, bytes});
+    }
+    return cudaSuccess;
+}
+
+void twtable_free_all(Context* c) {
+    std::lock_guard<std::mutex> lk(c->twt_mu);
+    for (const Context::TwTable& t : c->twt) {
+        cudaFree(t.fwd);
+        budget_release(c, t.bytes);
+    }
+    c->twt.clear();
 }
 
 uint64_t carry_scratch_bytes(int logn) {
