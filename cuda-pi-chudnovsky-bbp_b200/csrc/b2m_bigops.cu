@@ -501,13 +501,60 @@ DV sqrt_approx(Scope& S, DV N, uint64_t k, uint64_t h) {
     return shr(S, trim(S, s), 0, 1);
 }
 
-// floor(sqrt(N)) for trimmed N: a Newton estimate, then the remainder
-// R = N - s^2 moves s until 0 <= R <= 2s.
+DV isqrt(Scope& S, DV N);
+
+// Y ~ 2^(64h) / sqrt(N_h), N_h = floor(N / 2^(32(2k - 2h))), by Newton on the
+// reciprocal square root, y <- y + y (1 - N y^2) / 2: three products a step
+// and no division. The seed (h <= 8) is floor((2^(64h) - 1) / isqrt(N_h))
+// from the exact root; each step starts from l = floor((h + 3) / 2) limbs.
+DV rsqrt_approx(Scope& S, DV N, uint64_t k, uint64_t h) {
+    const uint64_t drop = 2 * k - 2 * h;
+    DV Nh = N.n > drop ? DV{N.p + drop, N.n - drop} : DV{N.p, 0};
+    if (h <= 8) {
+        DV root = isqrt(S, Nh);
+        DV num = S.vec(2 * h);
+        ck(cudaMemsetAsync(num.p, 0xFF, 8 * h, S.s()), "cudaMemsetAsync");  // 2^(64h) - 1
+        DV q, r;
+        divmod(S, num, root, &q, &r);
+        return q;
+    }
+    const uint64_t l = (h + 3) / 2;
+    DV Y0 = shl(S, rsqrt_approx(S, N, k, l), h - l, 0);
+    DV U = mul(S, Nh, mul(S, Y0, Y0));  // ~ 2^(128h)
+    const uint64_t e = 4 * h;
+    DV E;
+    bool neg = false;
+    if (U.n <= e) {  // E = 2^(32e) - U >= 0
+        E = S.vec(e);
+        addsub(S, DV{U.p, 0}, U, E, true);
+    } else {  // U = 2^(32e) + E'
+        if (U.n != e + 1 || limb_at(S, U, e) != 1) {
+            set_error("Newton reciprocal square root diverged");
+            throw Err{B2M_ERR_INTERNAL};
+        }
+        E = {U.p, e};
+        neg = true;
+    }
+    DV corr = shr(S, mul(S, Y0, trim(S, E)), e, 1);  // Y0 |E| / 2^(32e + 1)
+    DV Y = S.vec(std::max(Y0.n, corr.n) + 1);
+    addsub(S, Y0, corr, Y, neg);
+    return trim(S, Y);
+}
+
+// floor(sqrt(N)) for trimmed N: an estimate -- N * Y / 2^(64k) from the
+// reciprocal square root above, or for small N the division-based Newton
+// root -- then the remainder R = N - s^2 moves s until 0 <= R <= 2s.
 DV isqrt(Scope& S, DV N) {
     if (N.n == 0) return N;
     if (N.n <= 4) return trim(S, upload(S, from128(isqrt128(to128(download(S, N))))));
     const uint64_t k = (N.n + 1) / 2;
-    DV s = sqrt_approx(S, N, k, k);
+    DV s;
+    if (N.n <= 16) {
+        s = sqrt_approx(S, N, k, k);
+    } else {
+        DV Y = rsqrt_approx(S, N, k, k);
+        s = shr(S, mul(S, N, Y), 2 * k, 0);
+    }
     DV SQ = mul(S, s, s);
     const uint64_t w = std::max(N.n, SQ.n) + 2;
     DV R = S.vec(w);
