@@ -310,47 +310,58 @@ DV mul(Scope& S, DV a, DV b) {
     unsigned long long h = 0;
     ck(cudaMemcpyAsync(&h, d_len, 8, cudaMemcpyDeviceToHost, S.s()), "D2H");
     ck(cudaStreamSynchronize(S.s()), "cudaStreamSynchronize");
-    const b2m_status e = take_device_error(c);
-    if (e != B2M_OK) throw Err{e};
-    out.n = h;
+    out.n = h;  // the sticky device error word is checked once, when the call ends
     return out;
 }
 
 // ---------------------------------------------------------------------------- small host arithmetic
-// floor((2^(64h) - 1) / Y) for an h-limb Y whose top bit is set (binary long
-// division; only for the few-limb seed of the Newton reciprocal).
+// floor((2^(64h) - 1) / Y) for an h-limb Y whose top bit is set: schoolbook
+// long division on 32-bit digits (Knuth, TAOCP vol. 2, 4.3.1, algorithm D),
+// the numerator being 2h all-ones limbs. Seeds the Newton reciprocal.
 std::vector<u32> recip_small(const std::vector<u32>& Y) {
-    const size_t h = Y.size();
-    std::vector<u32> q(2 * h + 1, 0), r(h + 1, 0);
-    for (long bit = (long)(64 * h) - 1; bit >= 0; --bit) {
-        u32 carry = 1;  // the numerator's bits are all ones
-        for (size_t i = 0; i <= h; ++i) {
-            const u32 nc = r[i] >> 31;
-            r[i] = (r[i] << 1) | carry;
-            carry = nc;
-        }
-        bool ge = true;  // r >= Y ?
-        for (long i = (long)h; i >= 0; --i) {
-            const u32 yi = (size_t)i < h ? Y[i] : 0u;
-            if (r[i] != yi) {
-                ge = r[i] > yi;
-                break;
+    const size_t n = Y.size();
+    std::vector<u32> q(n + 1, 0);
+    if (n == 1) {
+        const u64 v = ~0ull / Y[0];
+        q[0] = (u32)v;
+        q[1] = (u32)(v >> 32);
+    } else {
+        std::vector<u32> un(2 * n + 1, 0xFFFFFFFFu);
+        un[2 * n] = 0;
+        const u64 b = 1ull << 32;
+        for (long j = (long)n; j >= 0; --j) {
+            const u64 num = ((u64)un[j + n] << 32) | un[j + n - 1];
+            u64 qhat = num / Y[n - 1], rhat = num % Y[n - 1];
+            while (qhat >= b || qhat * Y[n - 2] > ((rhat << 32) | un[j + n - 2])) {
+                --qhat;
+                rhat += Y[n - 1];
+                if (rhat >= b) break;
             }
-        }
-        if (ge) {
-            u64 bor = 0;
-            for (size_t i = 0; i <= h; ++i) {
-                const u64 d = (u64)r[i] - (i < h ? Y[i] : 0u) - bor;
-                r[i] = (u32)d;
-                bor = (d >> 63) & 1;
+            int64_t k = 0, t;
+            for (size_t i = 0; i < n; ++i) {
+                const u64 p = qhat * Y[i];
+                t = (int64_t)un[i + j] - k - (int64_t)(p & 0xFFFFFFFFull);
+                un[i + j] = (u32)t;
+                k = (int64_t)(p >> 32) - (t >> 32);
             }
-            q[bit / 32] |= 1u << (bit % 32);
+            t = (int64_t)un[j + n] - k;
+            un[j + n] = (u32)t;
+            if (t < 0) {
+                --qhat;
+                u64 c = 0;
+                for (size_t i = 0; i < n; ++i) {
+                    const u64 s = (u64)un[i + j] + Y[i] + c;
+                    un[i + j] = (u32)s;
+                    c = s >> 32;
+                }
+                un[j + n] += (u32)c;
+            }
+            q[j] = (u32)qhat;
         }
     }
     while (!q.empty() && q.back() == 0) q.pop_back();
     return q;
 }
-
 // floor(sqrt(v)) for v < 2^128 (bit by bit).
 unsigned __int128 isqrt128(unsigned __int128 v) {
     unsigned __int128 res = 0, bit = (unsigned __int128)1 << 126;
@@ -397,7 +408,7 @@ DV top_limbs(Scope& S, DV Bn, uint64_t h) {
 // the correct limbs; the +3 keeps a guard limb).
 DV recip(Scope& S, DV Bn, uint64_t h) {
     DV Y = top_limbs(S, Bn, h);
-    if (h <= 8) return trim(S, upload(S, recip_small(download(S, Y))));
+    if (h <= 32) return trim(S, upload(S, recip_small(download(S, Y))));
     const uint64_t l = (h + 3) / 2;
     DV Xl = recip(S, Bn, l);
     DV T = mul(S, Y, Xl);
@@ -805,21 +816,39 @@ std::string to_decimal(Scope& S, DV X) {
     uint64_t sin = std::max<uint64_t>(2 * P[J].n, X.n);
     DV in = copy(S, X, sin);
     uint64_t m = 1;
+    // Reciprocals R ~ 2^(32 E) / P_j: Newton for the top level only; below,
+    // 1/P_j = P_j / P_{j+1}, so R_j = P_j * R_{j+1} (more precise than level j
+    // needs), truncated to its top n + 4 limbs.
+    DV R;
+    uint64_t E = 0;
     for (int j = J; j > DC_LEAF_J; --j) {
         const DV Pj = P[j];
         const uint64_t n = Pj.n;
-        // reciprocal of P_j with the normalising shift folded in:
-        // q~ = floor(V * R / 2^(32 (L + n))) ~ floor(V / P_j)
-        const int sh = __builtin_clz(limb_at(S, Pj, n - 1));
-        DV Pn = sh ? shl(S, Pj, 0, sh) : Pj;
         const uint64_t L = n + 3;
-        DV R = recip(S, Pn, L);
-        if (sh) R = shl(S, R, 0, sh);
+        if (j == J) {
+            const int sh = __builtin_clz(limb_at(S, Pj, n - 1));
+            DV Pn = sh ? shl(S, Pj, 0, sh) : Pj;
+            R = recip(S, Pn, L);  // ~ 2^(32 (L + n)) / Pn, Pn = P_j 2^sh
+            if (sh) R = shl(S, R, 0, sh);
+            E = L + n;
+        } else {
+            R = mul(S, Pj, R);
+        }
+        if (R.n > L + 1) {  // keep the top L + 1 limbs
+            const uint64_t t = R.n - (L + 1);
+            R = {R.p + t, R.n - t};
+            E -= t;
+        }
+        // q~ = floor(V * R / 2^(32 E)) ~ floor(V / P_j), from V's top L + 1 limbs
         const uint64_t k = sin > L + 1 ? sin - (L + 1) : 0;
+        if (E < k) {
+            set_error("decimal conversion: reciprocal scale below the operand cut");
+            throw Err{B2M_ERR_INTERNAL};
+        }
         const uint64_t na = sin - k, sp = na + R.n;
         DV prod = S.vec(m * sp);
         batched_mul(S, in.p + k, sin, na, R.p, 0, R.n, prod.p, sp, m);
-        const uint64_t s = L + n - k, nq = n + 1;
+        const uint64_t s = E - k, nq = n + 1;
         DV qe = S.vec(m * nq);
         k_dc_extract<<<grid_for(m * nq), 256, 0, S.s()>>>(prod.p, sp, sp, s, nq, qe.p, m);
         ck(cudaGetLastError(), "k_dc_extract");
@@ -880,7 +909,7 @@ b2m_status run_op(b2m_stream stream, F&& f) {
     }
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_status(e, "cudaStreamSynchronize");
-    return B2M_OK;
+    return take_device_error(c);
 }
 
 void put(Scope& S, DV v, uint32_t* dst, uint64_t cap, uint64_t* len) {
