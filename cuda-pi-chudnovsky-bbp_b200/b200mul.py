@@ -209,6 +209,15 @@ def autotune(na: int, nb: int, stream: int = 0) -> list[dict]:
     return res
 
 
+_sig("b2m_selftest_wait_timeout", ctypes.c_int, [ctypes.c_void_p])
+
+
+def selftest_wait_timeout(stream: int = 0) -> int:
+    """Status of b2m_selftest_wait_timeout (8, B2M_ERR_DEVICE_TIMEOUT, when the
+    bounded device-side wait fires as designed)."""
+    return int(lib.b2m_selftest_wait_timeout(stream or None))
+
+
 _sig("b2m_set_plan", ctypes.c_int, [ctypes.POINTER(PlanDesc)])
 
 

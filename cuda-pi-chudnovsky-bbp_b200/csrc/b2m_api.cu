@@ -283,6 +283,36 @@ b2m_status b2m_plan_describe(uint64_t na, uint64_t nb, b2m_plan_desc* d) {
     return B2M_OK;
 }
 
+b2m_status b2m_selftest_wait_timeout(b2m_stream stream) {
+    Context* c = ctx();
+    if (!c) return B2M_ERR_NOT_INITIALIZED;
+    cudaSetDevice(c->device);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    // Two chunks of (zero) coefficients and their lookback slots, the ticket
+    // starting at 1: the one CTA launched takes chunk 1 and waits for chunk
+    // 0's flag, which nothing ever sets.
+    const uint64_t n = 2 * (uint64_t)CARRY_CHUNK;
+    auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
+    const uint64_t bc = al(8 * n), bo = al(4 * (n / 2)), bs = al(2 * sizeof(LookbackSlot)), bt = 256;
+    void* mem = nullptr;
+    cudaError_t e = cudaMallocAsync(&mem, bc + bo + bs + bt, s);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMallocAsync(self-test)");
+    unsigned char* b = static_cast<unsigned char*>(mem);
+    u32* ticket = reinterpret_cast<u32*>(b + bc + bo + bs);
+    static const u32 one = 1;
+    e = cudaMemsetAsync(mem, 0, bc + bo + bs + bt, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ticket, &one, 4, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = launch_carry(1, s, reinterpret_cast<const u64*>(b), reinterpret_cast<u32*>(b + bc), n / 2,
+                         reinterpret_cast<LookbackSlot*>(b + bc + bo), ticket,
+                         reinterpret_cast<unsigned long long*>(ticket + 2), c->d_err);
+    cudaFreeAsync(mem, s);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return cuda_status(e, "self-test launch");
+    return take_device_error(c);
+}
+
 b2m_status b2m_set_plan(const b2m_plan_desc* desc) {
     Context* c = ctx();
     if (!c) return B2M_ERR_NOT_INITIALIZED;

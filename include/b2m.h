@@ -121,6 +121,15 @@ b2m_status b2m_mul_device_noalloc(const uint32_t* d_a, uint64_t na, const uint32
  * raised by this library's kernels since the last check. */
 b2m_status b2m_stream_check(b2m_stream stream);
 
+/* No reference counterpart. Self-check of the device-side failure detection:
+ * runs the carry kernel on a crafted job whose only block waits on a
+ * predecessor that never publishes. The wait is bounded (a fixed number of
+ * polls, about half a second), so the kernel flags the error word and
+ * returns; the call reports B2M_ERR_DEVICE_TIMEOUT when that works as
+ * designed (B2M_OK would mean the bound did not fire) and leaves the context
+ * usable. Nothing faults, traps or hangs. */
+b2m_status b2m_selftest_wait_timeout(b2m_stream stream);
+
 /* ---- batched products ---------------------------------------------------------
  * No counterpart in the reference, whose tree (src/chudnovsky.cpp:64-102)
  * multiplies one pair at a time, each call paying its own allocation, copies

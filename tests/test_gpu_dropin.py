@@ -43,3 +43,22 @@ def test_reference_cli_digits_with_ntt_cuda_backend(tmp_path, digits):
     got = out.read_text().rstrip("\n")
     assert got[:102] == want["head"]
     assert hashlib.sha256(got.encode()).hexdigest() == want["sha256"]
+
+
+def test_bounded_device_wait_reports_timeout_and_context_survives(b2m_gpu):
+    """Failure detection without a fault: a carry block waits on a predecessor
+    that never publishes; the bounded wait gives up, the call reports
+    B2M_ERR_DEVICE_TIMEOUT, and the next product on the same context is exact."""
+    import time
+
+    import numpy as np
+
+    import oracle
+
+    t0 = time.perf_counter()
+    assert b2m_gpu.selftest_wait_timeout() == 8  # B2M_ERR_DEVICE_TIMEOUT
+    assert time.perf_counter() - t0 < 30
+    b2m_gpu.stream_check(0)  # the error word was read and cleared
+    a = np.arange(1, 5001, dtype=np.uint32)
+    b = np.arange(7, 3007, dtype=np.uint32)
+    assert np.array_equal(b2m_gpu.mul_ntt_cuda(a, b), oracle.mul_port(a, b))
