@@ -240,7 +240,7 @@ def run_ours(args) -> None:
     # every later product of this transform length uses the fastest.
     tune = [] if args.no_autotune else b200mul.autotune(na, nb, sp)
     plan = b200mul.plan_describe(na, nb)
-    n = 1 << plan["ntt_log2"]
+    n = plan["points"]
 
     def product():
         b200mul.mul_device(a.data_ptr(), na, b.data_ptr(), nb, out.data_ptr(), na + nb, olen.data_ptr(), sp)

@@ -72,7 +72,7 @@ _sig("b2m_mul_device_noalloc", ctypes.c_int,
 
 class PlanDesc(ctypes.Structure):
     _fields_ = [("ntt_log2", ctypes.c_uint32), ("npass", ctypes.c_uint32), ("logr", ctypes.c_uint32 * 3),
-                ("logc", ctypes.c_uint32 * 3), ("launches", ctypes.c_uint32)]
+                ("logc", ctypes.c_uint32 * 3), ("launches", ctypes.c_uint32), ("three", ctypes.c_uint32)]
 
 
 class KernelTime(ctypes.Structure):
@@ -80,7 +80,7 @@ class KernelTime(ctypes.Structure):
 
 
 KERNEL_KINDS = {1: "fwd_first", 2: "fwd_mid", 3: "fwd_last", 4: "fused_last", 5: "inv_mid", 6: "carry",
-                7: "mul_small"}
+                7: "mul_small", 8: "r3_fwd", 9: "r3_inv"}
 
 _sig("b2m_plan_describe", ctypes.c_int, [_u64, _u64, ctypes.POINTER(PlanDesc)])
 _sig("b2m_mul_device_traced", ctypes.c_int,
@@ -184,7 +184,8 @@ def plan_describe(na: int, nb: int) -> dict:
     d = PlanDesc()
     check(lib.b2m_plan_describe(na, nb, ctypes.byref(d)), "b2m_plan_describe")
     return {"ntt_log2": d.ntt_log2, "npass": d.npass, "logr": list(d.logr)[: max(d.npass, 1)],
-            "logc": list(d.logc)[: max(d.npass, 1)], "launches": d.launches}
+            "logc": list(d.logc)[: max(d.npass, 1)], "launches": d.launches, "three": d.three,
+            "points": (3 if d.three else 1) << d.ntt_log2}
 
 
 class TuneEntry(ctypes.Structure):

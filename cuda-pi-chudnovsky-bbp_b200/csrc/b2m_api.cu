@@ -227,7 +227,12 @@ uint64_t b2m_ntt_length(uint64_t na, uint64_t nb) { return ntt_length_of(na, nb)
 
 uint64_t b2m_workspace_bytes(uint64_t na, uint64_t nb) {
     if (na == 0 || nb == 0) return 0;
-    return workspace_bytes_for(ilog2_pow2(ntt_length_of(na, nb)));
+    Context* c = ctx();
+    int logn = 0, three = 0;
+    choose_length(2 * (na + nb), &logn, &three);
+    Plan p = c ? plan_for(c, logn) : make_plan(logn);
+    p.three = three;
+    return workspace_bytes_plan(p);
 }
 
 b2m_status b2m_mul_device(const uint32_t* d_a, uint64_t na, const uint32_t* d_b, uint64_t nb,
@@ -246,9 +251,9 @@ b2m_status b2m_mul_device(const uint32_t* d_a, uint64_t na, const uint32_t* d_b,
     b2m_status st = check_sizes(na, nb, &logn);
     if (st != B2M_OK) return st;
     cudaSetDevice(c->device);
-    const Plan p = plan_for(c, logn);
+    const Plan p = product_plan(c, na, nb);
     if (cudaError_t te = twtable_ensure(c, p, s)) return cuda_status(te, "twiddle table");
-    const uint64_t wsb = workspace_bytes_for(logn);
+    const uint64_t wsb = workspace_bytes_plan(p);
     if (!budget_reserve(c, wsb)) {
         set_error("HBM budget exhausted");
         return B2M_ERR_OUT_OF_MEMORY;
@@ -272,8 +277,12 @@ b2m_status b2m_plan_describe(uint64_t na, uint64_t nb, b2m_plan_desc* d) {
     b2m_status st = check_sizes(na, nb, &logn);
     if (st != B2M_OK) return st;
     Context* c = ctx();
-    const Plan p = c ? plan_for(c, logn) : make_plan(logn);
-    d->ntt_log2 = (uint32_t)logn;
+    int l = 0, three = 0;
+    choose_length(2 * (na + nb), &l, &three);
+    Plan p = c ? plan_for(c, l) : make_plan(l);
+    p.three = three;
+    d->ntt_log2 = (uint32_t)l;
+    d->three = (uint32_t)three;
     d->npass = (uint32_t)p.npass;
     for (int k = 0; k < 3; ++k) {
         d->logr[k] = (uint32_t)p.logr[k];
@@ -342,9 +351,12 @@ b2m_status b2m_autotune(uint64_t na, uint64_t nb, b2m_stream stream, b2m_tune_en
     if (st != B2M_OK) return st;
     cudaSetDevice(c->device);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const std::vector<Plan> cands = plan_candidates(logn);
+    int three = 0;
+    choose_length(2 * (na + nb), &logn, &three);  // candidates for the (sub-)transform length
+    std::vector<Plan> cands = plan_candidates(logn);
+    for (Plan& cp : cands) cp.three = three;
     auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
-    const uint64_t ba = al(4 * na), bb = al(4 * nb), bo = al(4 * (na + nb)), wsb = al(workspace_bytes_for(logn));
+    const uint64_t ba = al(4 * na), bb = al(4 * nb), bo = al(4 * (na + nb)), wsb = al(workspace_bytes_plan(cands[0]));
     const uint64_t need = ba + bb + bo + 256 + wsb;
     if (!budget_reserve(c, need)) {
         set_error("HBM budget exhausted");
@@ -397,6 +409,7 @@ b2m_status b2m_autotune(uint64_t na, uint64_t nb, b2m_stream stream, b2m_tune_en
                 o.plan.logc[k] = (uint32_t)p.logc[k];
             }
             o.plan.launches = (uint32_t)plan_launches(p);
+            o.plan.three = (uint32_t)p.three;
             o.ms = ms[1];
             o.chosen = 0;
         }
@@ -410,7 +423,9 @@ b2m_status b2m_autotune(uint64_t na, uint64_t nb, b2m_stream stream, b2m_tune_en
     if (e != cudaSuccess) return cuda_status(e, "autotune");
     st = take_device_error(c);
     if (st != B2M_OK) return st;
-    set_tuned(c, logn, cands[best_i]);
+    Plan kept = cands[best_i];
+    kept.three = 0;  // tuned plans are kept per power-of-two length
+    set_tuned(c, logn, kept);
     if (best_i < cnt) out[best_i].chosen = 1;
     if (n) *n = cnt;
     return B2M_OK;
@@ -428,9 +443,9 @@ b2m_status b2m_mul_device_traced(const uint32_t* d_a, uint64_t na, const uint32_
     if (st != B2M_OK) return st;
     cudaSetDevice(c->device);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const Plan p = plan_for(c, logn);
+    const Plan p = product_plan(c, na, nb);
     if (cudaError_t te = twtable_ensure(c, p, s)) return cuda_status(te, "twiddle table");
-    const uint64_t wsb = workspace_bytes_for(logn);
+    const uint64_t wsb = workspace_bytes_plan(p);
     if (!budget_reserve(c, wsb)) {
         set_error("HBM budget exhausted");
         return B2M_ERR_OUT_OF_MEMORY;
@@ -487,10 +502,10 @@ b2m_status b2m_mul_host(const uint32_t* a, uint64_t na, const uint32_t* b, uint6
     if (st != B2M_OK) return st;
     std::lock_guard<std::mutex> lk(c->host_mu);
     cudaSetDevice(c->device);
-    const Plan p = plan_for(c, logn);
+    const Plan p = product_plan(c, na, nb);
     auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
     const uint64_t ba = al(4 * na), bb = al(4 * nb), bo = al(4 * (na + nb)), bl = 256;
-    const uint64_t wsb = workspace_bytes_for(logn);
+    const uint64_t wsb = workspace_bytes_plan(p);
     const uint64_t need = ba + bb + bo + bl + wsb;
     if (need > c->host_dev_cap) {
         if (c->host_dev) {

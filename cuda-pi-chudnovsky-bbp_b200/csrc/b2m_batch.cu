@@ -94,6 +94,7 @@ static void free_batch(b2m_batch* bt) {
 // Time every candidate plan of bucket b on its own jobs; keep the fastest.
 static cudaError_t autotune_bucket(b2m_batch* bt, Bucket& b, cudaStream_t s) {
     Context* c = bt->ctx;
+    if (b.plan.three) return cudaSuccess;  // radix-3 buckets run the sub-length's current plan
     {
         std::lock_guard<std::mutex> lk(c->tune_mu);
         if (c->has_tuned[b.logn]) {
@@ -147,7 +148,7 @@ b2m_status b2m_batch_create(const b2m_job* jobs, uint64_t njobs, uint32_t flags,
         return B2M_ERR_INVALID_ARGUMENT;
     *out = nullptr;
     // Validate and bucket.
-    std::map<int, std::vector<unsigned>> by_logn;  // logn -> job indices
+    std::map<uint64_t, std::vector<unsigned>> by_pts;  // transform points -> job indices
     std::vector<unsigned> empty;
     for (uint64_t i = 0; i < njobs; ++i) {
         const b2m_job& j = jobs[i];
@@ -158,10 +159,11 @@ b2m_status b2m_batch_create(const b2m_job* jobs, uint64_t njobs, uint32_t flags,
         }
         if (!j.out) return B2M_ERR_INVALID_ARGUMENT;
         if (j.out_cap < j.na + j.nb) return B2M_ERR_OUTPUT_TOO_SMALL;
-        int logn;
+        int logn, three;
         b2m_status st = check_sizes(j.na, j.nb, &logn);
         if (st != B2M_OK) return st;
-        by_logn[logn].push_back((unsigned)i);
+        choose_length(2 * (j.na + j.nb), &logn, &three);
+        by_pts[(three ? 3ull : 1ull) << logn].push_back((unsigned)i);
     }
     cudaSetDevice(c->device);
     b2m_batch* bt = new b2m_batch();
@@ -171,10 +173,10 @@ b2m_status b2m_batch_create(const b2m_job* jobs, uint64_t njobs, uint32_t flags,
     const uint64_t tab = al(njobs * sizeof(ProdJob));
     const uint64_t lens = al(njobs * sizeof(uint64_t));
     uint64_t bufs = 0, scr = 0;
-    for (auto& kv : by_logn) {
-        if (kv.first <= SMALL_MAX_LOGN) continue;
-        bufs += kv.second.size() * 2 * (8ull << kv.first);
-        scr += kv.second.size() * al(carry_scratch_bytes(kv.first));
+    for (auto& kv : by_pts) {
+        if (kv.first <= (1ull << SMALL_MAX_LOGN)) continue;
+        bufs += kv.second.size() * 2 * 8 * kv.first;
+        scr += kv.second.size() * al(carry_scratch_bytes_n(kv.first));
     }
     bt->dbytes = tab + lens + bufs + scr;
     if (!budget_reserve(c, bt->dbytes)) {
@@ -211,24 +213,29 @@ b2m_status b2m_batch_create(const b2m_job* jobs, uint64_t njobs, uint32_t flags,
         return p;
     };
     constexpr unsigned MAX_GRID_Y = 65535;  // a bucket launch covers at most this many jobs
-    for (auto it = by_logn.rbegin(); it != by_logn.rend(); ++it) {
-      const uint64_t n = 1ull << it->first;
+    for (auto it = by_pts.rbegin(); it != by_pts.rend(); ++it) {
+      const uint64_t n = it->first;
+      const int three = (n & (n - 1)) ? 1 : 0;  // 3 * 2^k is no power of two
+      const uint64_t sub = three ? n / 3 : n;      // the (sub-)transform length 2^k
+      int lg = 0;
+      while ((1ull << lg) < sub) ++lg;
       for (size_t off = 0; off < it->second.size(); off += MAX_GRID_Y) {
         Bucket b;
-        b.logn = it->first;
+        b.logn = lg;
         b.plan = plan_for(c, b.logn);
+        b.plan.three = three;
         b.first = (unsigned)hj.size();
         b.njobs = (unsigned)std::min<size_t>(MAX_GRID_Y, it->second.size() - off);
         for (size_t k = off; k < off + b.njobs; ++k) {
             const unsigned i = it->second[k];
             ProdJob p = mk(i);
-            if (b.logn > SMALL_MAX_LOGN) {
+            if (n > (1ull << SMALL_MAX_LOGN)) {
                 p.bufA = reinterpret_cast<u64*>(pbuf);
                 p.bufB = p.bufA + n;
                 pbuf += 2 * 8 * n;
                 p.slots = reinterpret_cast<LookbackSlot*>(pscr);
                 p.ticket = reinterpret_cast<u32*>(pscr + (n / CARRY_CHUNK) * sizeof(LookbackSlot));
-                pscr += al(carry_scratch_bytes(b.logn));
+                pscr += al(carry_scratch_bytes_n(n));
             }
             hj.push_back(p);
         }

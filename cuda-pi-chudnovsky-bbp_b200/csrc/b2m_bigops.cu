@@ -301,10 +301,10 @@ DV mul(Scope& S, DV a, DV b) {
     const b2m_status st = check_sizes(a.n, b.n, &logn);
     if (st != B2M_OK) throw Err{st};
     Context* c = S.c();
-    const Plan p = plan_for(c, logn);
+    const Plan p = product_plan(c, a.n, b.n);
     ck(twtable_ensure(c, p, S.s()), "twiddle table");
     DV out = S.vec(a.n + b.n);
-    void* ws = p.npass ? S.raw(workspace_bytes_for(logn)) : nullptr;
+    void* ws = p.npass ? S.raw(workspace_bytes_plan(p)) : nullptr;
     uint64_t* d_len = reinterpret_cast<uint64_t*>(S.word() + 2);
     ck(launch_product(a.p, a.n, b.p, b.n, out.p, d_len, ws, p, c->tw, c->d_err, S.s()), "product");
     unsigned long long h = 0;
@@ -607,7 +607,7 @@ constexpr int DC_LEAF_LIMBS = 8;  // 10^72 < 2^240
 constexpr int DC_LEAF_GROUPS = 8;
 
 __global__ void k_dc_jobs(const u32* a, u64 sa, u64 na, const u32* b, u64 sb, u64 nb, u32* out, u64 so,
-                          unsigned long long* lens, ProdJob* jobs, u64 njobs, unsigned char* ws, u64 wss, int logn) {
+                          unsigned long long* lens, ProdJob* jobs, u64 njobs, unsigned char* ws, u64 wss, u64 npts) {
     const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= njobs) return;
     ProdJob J{};
@@ -618,7 +618,7 @@ __global__ void k_dc_jobs(const u32* a, u64 sa, u64 na, const u32* b, u64 sb, u6
     J.out = out + i * so;
     J.out_len = lens + i;
     if (wss) {
-        const u64 n = 1ull << logn;
+        const u64 n = npts;
         unsigned char* w = ws + i * wss;
         J.bufA = reinterpret_cast<u64*>(w);
         J.bufB = J.bufA + n;
@@ -645,9 +645,10 @@ void batched_mul(Scope& S, const u32* a, uint64_t sa, uint64_t na, const u32* b,
     const b2m_status st = check_sizes(na, nb, &logn);
     if (st != B2M_OK) throw Err{st};
     Context* c = S.c();
-    const Plan p = plan_for(c, logn);
+    const Plan p = product_plan(c, na, nb);
     ck(twtable_ensure(c, p, S.s()), "twiddle table");
-    const uint64_t wss = p.npass ? ((workspace_bytes_for(logn) + 255) & ~255ull) : 0;
+    const uint64_t npts = plan_points(p);
+    const uint64_t wss = p.npass ? ((workspace_bytes_plan(p) + 255) & ~255ull) : 0;
     // at most 65535 jobs a launch, and at most ~1 GiB of transform workspace
     uint64_t chunk = 65535;
     if (wss) chunk = std::max<uint64_t>(1, std::min<uint64_t>(chunk, (1ull << 30) / wss));
@@ -657,8 +658,8 @@ void batched_mul(Scope& S, const u32* a, uint64_t sa, uint64_t na, const u32* b,
         unsigned long long* lens = static_cast<unsigned long long*>(S.raw(nj * 8));
         unsigned char* ws = wss ? static_cast<unsigned char*>(S.raw(nj * wss)) : nullptr;
         k_dc_jobs<<<(unsigned)((nj + 255) / 256), 256, 0, S.s()>>>(a + off * sa, sa, na, b + off * sb, sb, nb,
-                                                                  out + off * so, so, lens, jobs, nj, ws, wss, logn);
-        if (wss) k_dc_zero_ws<<<(unsigned)nj, 256, 0, S.s()>>>(jobs, nj, carry_scratch_bytes(logn) / 8);
+                                                                  out + off * so, so, lens, jobs, nj, ws, wss, npts);
+        if (wss) k_dc_zero_ws<<<(unsigned)nj, 256, 0, S.s()>>>(jobs, nj, carry_scratch_bytes_n(npts) / 8);
         ck(cudaGetLastError(), "job tables");
         ck(launch_bucket(p, jobs, (unsigned)nj, c->tw, c->d_err, S.s()), "batched product");
     }

@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(SCHOOL_WARPS * 32) k_bs_school(LevelView L, Le
 
 // Job tables of one product kind for the NTT buckets.
 __global__ void k_bs_build_jobs(LevelView L, LevelView Ln, ScratchXY S, u64 m2, int kind, ProdJob* jobs,
-                                unsigned char* ntt_ws, u64 ws_stride, u64 nlogn) {
+                                unsigned char* ntt_ws, u64 ws_stride, u64 npts) {
     const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m2) return;
     const MergeProd p = merge_prod(L, Ln, S, i, kind);
@@ -193,7 +193,7 @@ __global__ void k_bs_build_jobs(LevelView L, LevelView Ln, ScratchXY S, u64 m2, 
     J.out = p.out;
     J.out_len = reinterpret_cast<unsigned long long*>(p.out_len);
     if (ntt_ws) {
-        const u64 n = 1ull << nlogn;
+        const u64 n = npts;
         unsigned char* w = ntt_ws + i * ws_stride;
         J.bufA = reinterpret_cast<u64*>(w);
         J.bufB = J.bufA + n;
@@ -468,11 +468,14 @@ static cudaError_t merge_level(Context* c, const LevelView& L, const uint64_t mx
     std::vector<uint64_t> tmpb;
     for (int k = 0; k < 4 && m2 && e == cudaSuccess; ++k) {
         if ((school_mask >> k) & 1) continue;
-        const int logn = ceil_log2(2 * cap[k]);
-        if (logn > MAX_LOGN) return cudaErrorInvalidValue;
-        const Plan p = plan_for(c, logn);
+        if (ceil_log2(2 * cap[k]) > MAX_LOGN) return cudaErrorInvalidValue;
+        int logn = 0, three = 0;
+        choose_length(2 * cap[k], &logn, &three);
+        Plan p = plan_for(c, logn);
+        p.three = three;
+        const uint64_t npts = plan_points(p);
         if ((e = twtable_ensure(c, p, s)) != cudaSuccess) break;
-        const uint64_t wss = logn > SMALL_MAX_LOGN ? al(workspace_bytes_for(logn)) : 0;
+        const uint64_t wss = p.npass ? al(workspace_bytes_plan(p)) : 0;
         const uint64_t tb = al(m2 * sizeof(ProdJob)) + m2 * wss;
         void* t = nullptr;
         if (!budget_reserve(c, tb)) {
@@ -487,9 +490,9 @@ static cudaError_t merge_level(Context* c, const LevelView& L, const uint64_t mx
         tmpb.push_back(tb);
         ProdJob* jobs = static_cast<ProdJob*>(t);
         unsigned char* ws = wss ? static_cast<unsigned char*>(t) + al(m2 * sizeof(ProdJob)) : nullptr;
-        k_bs_build_jobs<<<(unsigned)((m2 + 255) / 256), 256, 0, s>>>(L, *Ln, S, m2, k, jobs, ws, wss, logn);
+        k_bs_build_jobs<<<(unsigned)((m2 + 255) / 256), 256, 0, s>>>(L, *Ln, S, m2, k, jobs, ws, wss, npts);
         if (wss) {
-            const uint64_t scratch_words = carry_scratch_bytes(logn) / 8;
+            const uint64_t scratch_words = carry_scratch_bytes_n(npts) / 8;
             k_bs_zero_ws<<<(unsigned)m2, 256, 0, s>>>(jobs, m2, scratch_words);
         }
         if ((e = cudaGetLastError()) != cudaSuccess) break;

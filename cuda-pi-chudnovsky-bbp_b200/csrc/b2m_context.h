@@ -50,6 +50,16 @@ inline Plan plan_for(Context* c, int logn) {
     std::lock_guard<std::mutex> lk(c->tune_mu);
     return c->has_tuned[logn] ? c->tuned[logn] : make_plan(logn);
 }
+// The plan of an na x nb product: 2^L points, or 3 * 2^(L-2) when that holds
+// the 2(na + nb) digits (choose_length), its sub-transform the tuned or
+// default plan of that length.
+inline Plan product_plan(Context* c, uint64_t na, uint64_t nb) {
+    int logn = 0, three = 0;
+    choose_length(2 * (na + nb), &logn, &three);
+    Plan p = plan_for(c, logn);
+    p.three = three;
+    return p;
+}
 inline void set_tuned(Context* c, int logn, const Plan& p) {
     std::lock_guard<std::mutex> lk(c->tune_mu);
     c->tuned[logn] = p;

@@ -34,7 +34,22 @@ struct Plan {
     int npass = 0;   // 0 = single-CTA multiply
     int logr[3] = {0, 0, 0};
     int logc[3] = {0, 0, 0};
+    // 1: 3 * 2^logn points -- a radix-3 step (ntt_radix3.cu) around three
+    // 2^logn-point transforms that run the passes above (npass >= 2).
+    int three = 0;
 };
+
+// Points of a plan's transform, and the workspace and carry scratch a
+// product with that plan needs.
+inline uint64_t plan_points(const Plan& p) { return (p.three ? 3ull : 1ull) << p.logn; }
+uint64_t carry_scratch_bytes_n(uint64_t points);
+uint64_t workspace_bytes_plan(const Plan& p);
+// A transform of 3 * 2^k points is used when k >= RADIX3_MIN_LOG and it still
+// holds the product's digits (fewer points than the next power of two).
+constexpr int RADIX3_MIN_LOG = 14;
+// Log2 of the sub-transform and the radix-3 choice for `digits` points of
+// convolution output (2na + 2nb): three = 1 when 3 * 2^(L-2) >= digits.
+void choose_length(uint64_t digits, int* logn, int* three);
 
 Plan make_plan(int logn);
 Plan make_plan_custom(int logn, int r0, int tile);
@@ -117,6 +132,10 @@ struct PassGeo {
     // (logm, logr); null: the kernels build each twiddle from u1 * u2.
     const u64* tfwd = nullptr;
     const u64* tinv = nullptr;
+    // Radix-3 plans: grid z runs over the three sub-transforms, zstride
+    // elements apart (1 and 0 otherwise).
+    unsigned zdim = 1;
+    u64 zstride = 0;
 };
 PassGeo pass_geo(const Plan& p, int k);
 
@@ -145,6 +164,10 @@ cudaError_t launch_fwd_last(int logr, const PassGeo& g, cudaStream_t s, u64* buf
                             const ProdJob* jobs = nullptr, unsigned njobs = 1);
 cudaError_t launch_fused_last(int logr, const PassGeo& g, cudaStream_t s, u64* bbuf, const u64* aspec, u64 ninv,
                               const RootTables& tw, const ProdJob* jobs = nullptr, unsigned njobs = 1);
+cudaError_t launch_r3_fwd(cudaStream_t s, const u32* limbs, u64 ndig, u64* out, int logm, const RootTables& tw,
+                          const ProdJob* jobs = nullptr, unsigned njobs = 1, int operand = 0);
+cudaError_t launch_r3_inv(cudaStream_t s, u64* buf, int logm, const RootTables& tw, const ProdJob* jobs = nullptr,
+                          unsigned njobs = 1);
 cudaError_t launch_mul_small(int logn, const PassGeo& g, cudaStream_t s, const u32* a, u64 na, const u32* b, u64 nb,
                              u32* out, u64 nout, unsigned long long* out_len, u64 ninv, const RootTables& tw,
                              const ProdJob* jobs = nullptr, unsigned njobs = 1);

@@ -86,7 +86,7 @@ extern "C" b2m_status b2m_mul_device_noalloc(const uint32_t* d_a, uint64_t na, c
     if (e != cudaSuccess) return cuda_status(e, "cudaSetDevice");
     void* ws = nullptr;
     if ((st = noalloc_scratch(c->device, &ws)) != B2M_OK) return st;
-    const Plan p = plan_for(c, logn);
+    const Plan p = product_plan(c, na, nb);  // at most 2^20 points: within the static scratch
     e = launch_product(d_a, na, d_b, nb, d_out, d_out_len, ws, p, c->tw, c->d_err, s);
     return cuda_status(e, "kernel launch");
 }

@@ -90,7 +90,9 @@ static uint64_t now_ns() {
 
 struct Req {
     b2m_request r{};
-    int logn = 0;
+    int logn = 0;       // log2 of the (sub-)transform length
+    int three = 0;      // 1: 3 * 2^logn points
+    uint64_t pts = 0;   // transform points
     int32_t state = 0;  // 0 queued, 1 on the GPU, 2 done, 3 failed
     b2m_status status = B2M_OK;
     u32* a = nullptr;  // device operands (owned when generated)
@@ -163,13 +165,13 @@ static cudaError_t launch_dispatch(b2m_server* S, Slot& sl, std::vector<Req>& rv
     // Dispatch block: [job table][lengths][residues][buffers][carry scratch].
     std::vector<size_t> order(n);
     for (size_t i = 0; i < n; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return rs[x]->logn > rs[y]->logn; });
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return rs[x]->pts > rs[y]->pts; });
     const uint64_t tab = al(n * sizeof(ProdJob)), lens = al(n * 8), res = al(n * RES_WORDS * 8);
     uint64_t bufs = 0, scr = 0;
     for (Req* q : rs)
-        if (q->logn > SMALL_MAX_LOGN) {
-            bufs += 2 * (8ull << q->logn);
-            scr += al(carry_scratch_bytes(q->logn));
+        if (q->pts > (1ull << SMALL_MAX_LOGN)) {
+            bufs += 2 * 8 * q->pts;
+            scr += al(carry_scratch_bytes_n(q->pts));
         }
     sl.block_bytes = tab + lens + res + bufs + scr;
     if (sl.block_bytes > sl.arena_cap) {
@@ -218,14 +220,14 @@ static cudaError_t launch_dispatch(b2m_server* S, Slot& sl, std::vector<Req>& rv
         J.na = q->r.na;
         J.nb = q->r.nb;
         J.out_len = reinterpret_cast<unsigned long long*>(dlens + k);
-        if (q->logn > SMALL_MAX_LOGN) {
-            const uint64_t nn = 1ull << q->logn;
+        if (q->pts > (1ull << SMALL_MAX_LOGN)) {
+            const uint64_t nn = q->pts;
             J.bufA = reinterpret_cast<u64*>(pbuf);
             J.bufB = J.bufA + nn;
             pbuf += 16 * nn;
             J.slots = reinterpret_cast<LookbackSlot*>(pscr);
             J.ticket = reinterpret_cast<u32*>(pscr + (nn / CARRY_CHUNK) * sizeof(LookbackSlot));
-            pscr += al(carry_scratch_bytes(q->logn));
+            pscr += al(carry_scratch_bytes_n(nn));
         }
         hj[k] = J;
     }
@@ -238,10 +240,11 @@ static cudaError_t launch_dispatch(b2m_server* S, Slot& sl, std::vector<Req>& rv
         return e;
     // Buckets: consecutive equal transform lengths.
     for (size_t k0 = 0; k0 < n;) {
-        const int logn = rs[order[k0]]->logn;
+        const uint64_t pts = rs[order[k0]]->pts;
         size_t k1 = k0;
-        while (k1 < n && rs[order[k1]]->logn == logn && k1 - k0 < 65535) ++k1;
-        const Plan p = plan_for(S->c, logn);
+        while (k1 < n && rs[order[k1]]->pts == pts && k1 - k0 < 65535) ++k1;
+        Plan p = plan_for(S->c, rs[order[k0]]->logn);
+        p.three = rs[order[k0]]->three;
         if ((e = twtable_ensure(S->c, p, s)) != cudaSuccess) return e;
         if ((e = launch_bucket(p, djobs + k0, (unsigned)(k1 - k0), S->c->tw, S->c->d_err, s)) != cudaSuccess) return e;
         // Residue check of the bucket's products, its grid sized to the
@@ -351,7 +354,7 @@ static void scheduler(b2m_server* S) {
             // launch_dispatch sorted the jobs by size: record ids in that order
             std::vector<size_t> order(rs.size());
             for (size_t i = 0; i < order.size(); ++i) order[i] = i;
-            std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return rs[x].logn > rs[y].logn; });
+            std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return rs[x].pts > rs[y].pts; });
             sl.ids.resize(rs.size());
             for (size_t k = 0; k < order.size(); ++k) sl.ids[k] = ids[order[k]];
             sl.busy = true;
@@ -412,7 +415,8 @@ b2m_status b2m_server_submit(b2m_server* S, const b2m_request* req, uint64_t* ti
     if (st != B2M_OK) return st;
     Req q;
     q.r = r;
-    q.logn = logn;
+    choose_length(2 * (r.na + r.nb), &q.logn, &q.three);
+    q.pts = (q.three ? 3ull : 1ull) << q.logn;
     q.own_a = r.a == nullptr;
     q.own_b = r.b == nullptr;
     q.own_out = r.out == nullptr;
@@ -421,7 +425,7 @@ b2m_status b2m_server_submit(b2m_server* S, const b2m_request* req, uint64_t* ti
     q.out = r.out;
     auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
     q.own_bytes = (q.own_a ? al(4 * r.na) : 0) + (q.own_b ? al(4 * r.nb) : 0) + (q.own_out ? al(4 * (r.na + r.nb)) : 0);
-    q.ws_bytes = (logn > SMALL_MAX_LOGN ? 2 * (8ull << logn) + al(carry_scratch_bytes(logn)) : 0) + 256;
+    q.ws_bytes = (q.pts > (1ull << SMALL_MAX_LOGN) ? 2 * 8 * q.pts + al(carry_scratch_bytes_n(q.pts)) : 0) + 256;
     if (q.own_bytes + q.ws_bytes > S->cfg.hbm_budget_bytes) {
         set_error("request larger than the server's HBM budget");
         return B2M_ERR_OUT_OF_MEMORY;

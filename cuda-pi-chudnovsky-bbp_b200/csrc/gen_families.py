@@ -33,22 +33,22 @@ FAMILIES = [
         ("k_fwd_mid", COL, "launch_fwd_mid",
          "(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw, const ProdJob* jobs, "
          "unsigned njobs, int operand)",
-         "(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand)", "dim3(g.grid, njobs)")]),
+         "(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride)", "dim3(g.grid, njobs, g.zdim)")]),
     ("ntt_fam_inv.cu", "non-last inverse passes", "inv", [
         ("k_inv_mid", COL, "launch_inv_mid",
          "(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw, const ProdJob* jobs, "
          "unsigned njobs)",
-         "(buf, g.logs, g.logm, tw, g.tinv, jobs)", "dim3(g.grid, njobs)")]),
+         "(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride)", "dim3(g.grid, njobs, g.zdim)")]),
     ("ntt_fam_last.cu", "last forward pass of operand A", "last", [
         ("k_fwd_last", ROW, "launch_fwd_last",
          "(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw, const ProdJob* jobs, "
          "unsigned njobs)",
-         "(buf, tw, jobs)", "dim3(g.grid, njobs)")]),
+         "(buf, tw, jobs, g.zstride)", "dim3(g.grid, njobs, g.zdim)")]),
     ("ntt_fam_fused.cu", "fused last pass of operand B (forward, pointwise, inverse)", "fused", [
         ("k_fused_last", ROW, "launch_fused_last",
          "(int logr, const PassGeo& g, cudaStream_t s, u64* bbuf, const u64* aspec, u64 ninv, "
          "const RootTables& tw, const ProdJob* jobs, unsigned njobs)",
-         "(bbuf, aspec, ninv, tw, jobs)", "dim3(g.grid, njobs)")]),
+         "(bbuf, aspec, ninv, tw, jobs, g.zstride)", "dim3(g.grid, njobs, g.zdim)")]),
 ]
 
 SMALL = ("ntt_fam_small.cu", "single-CTA products, N <= 2^13", "small", "k_mul_small", range(2, 14),

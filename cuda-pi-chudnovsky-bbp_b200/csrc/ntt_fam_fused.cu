@@ -8,27 +8,27 @@ namespace b2m {
 
 cudaError_t launch_fused_last(int logr, const PassGeo& g, cudaStream_t s, u64* bbuf, const u64* aspec, u64 ninv, const RootTables& tw, const ProdJob* jobs, unsigned njobs) {
     switch (logr * 32 + g.logc) {
-        case 229: k_fused_last<7, 5><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 260: k_fused_last<8, 4><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 291: k_fused_last<9, 3><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 322: k_fused_last<10, 2><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 353: k_fused_last<11, 1><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 384: k_fused_last<12, 0><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 230: k_fused_last<7, 6><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 261: k_fused_last<8, 5><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 292: k_fused_last<9, 4><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 323: k_fused_last<10, 3><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 354: k_fused_last<11, 2><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 385: k_fused_last<12, 1><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 416: k_fused_last<13, 0><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 231: k_fused_last<7, 7><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 262: k_fused_last<8, 6><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 293: k_fused_last<9, 5><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 324: k_fused_last<10, 4><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 355: k_fused_last<11, 3><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 386: k_fused_last<12, 2><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 417: k_fused_last<13, 1><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
-        case 448: k_fused_last<14, 0><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs); break;
+        case 229: k_fused_last<7, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 260: k_fused_last<8, 4><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 291: k_fused_last<9, 3><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 322: k_fused_last<10, 2><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 353: k_fused_last<11, 1><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 384: k_fused_last<12, 0><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 230: k_fused_last<7, 6><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 261: k_fused_last<8, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 292: k_fused_last<9, 4><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 323: k_fused_last<10, 3><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 354: k_fused_last<11, 2><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 385: k_fused_last<12, 1><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 416: k_fused_last<13, 0><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 231: k_fused_last<7, 7><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 262: k_fused_last<8, 6><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 293: k_fused_last<9, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 324: k_fused_last<10, 4><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 355: k_fused_last<11, 3><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 386: k_fused_last<12, 2><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 417: k_fused_last<13, 1><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 448: k_fused_last<14, 0><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
         default: return cudaErrorInvalidConfiguration;
     }
     return cudaGetLastError();

@@ -8,24 +8,24 @@ namespace b2m {
 
 cudaError_t launch_inv_mid(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw, const ProdJob* jobs, unsigned njobs) {
     switch (logr * 32 + g.logc) {
-        case 229: k_inv_mid<7, 5><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 260: k_inv_mid<8, 4><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 291: k_inv_mid<9, 3><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 322: k_inv_mid<10, 2><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 353: k_inv_mid<11, 1><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 384: k_inv_mid<12, 0><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 230: k_inv_mid<7, 6><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 261: k_inv_mid<8, 5><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 292: k_inv_mid<9, 4><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 323: k_inv_mid<10, 3><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 354: k_inv_mid<11, 2><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 385: k_inv_mid<12, 1><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 231: k_inv_mid<7, 7><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 262: k_inv_mid<8, 6><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 293: k_inv_mid<9, 5><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 324: k_inv_mid<10, 4><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 355: k_inv_mid<11, 3><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
-        case 386: k_inv_mid<12, 2><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs); break;
+        case 229: k_inv_mid<7, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 260: k_inv_mid<8, 4><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 291: k_inv_mid<9, 3><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 322: k_inv_mid<10, 2><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 353: k_inv_mid<11, 1><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 384: k_inv_mid<12, 0><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 230: k_inv_mid<7, 6><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 261: k_inv_mid<8, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 292: k_inv_mid<9, 4><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 323: k_inv_mid<10, 3><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 354: k_inv_mid<11, 2><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 385: k_inv_mid<12, 1><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 231: k_inv_mid<7, 7><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 262: k_inv_mid<8, 6><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 293: k_inv_mid<9, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 324: k_inv_mid<10, 4><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 355: k_inv_mid<11, 3><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 386: k_inv_mid<12, 2><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
         default: return cudaErrorInvalidConfiguration;
     }
     return cudaGetLastError();

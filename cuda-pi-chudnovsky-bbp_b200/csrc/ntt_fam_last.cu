@@ -8,27 +8,27 @@ namespace b2m {
 
 cudaError_t launch_fwd_last(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw, const ProdJob* jobs, unsigned njobs) {
     switch (logr * 32 + g.logc) {
-        case 229: k_fwd_last<7, 5><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 260: k_fwd_last<8, 4><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 291: k_fwd_last<9, 3><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 322: k_fwd_last<10, 2><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 353: k_fwd_last<11, 1><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 384: k_fwd_last<12, 0><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 230: k_fwd_last<7, 6><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 261: k_fwd_last<8, 5><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 292: k_fwd_last<9, 4><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 323: k_fwd_last<10, 3><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 354: k_fwd_last<11, 2><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 385: k_fwd_last<12, 1><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 416: k_fwd_last<13, 0><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 231: k_fwd_last<7, 7><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 262: k_fwd_last<8, 6><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 293: k_fwd_last<9, 5><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 324: k_fwd_last<10, 4><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 355: k_fwd_last<11, 3><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 386: k_fwd_last<12, 2><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 417: k_fwd_last<13, 1><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
-        case 448: k_fwd_last<14, 0><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, tw, jobs); break;
+        case 229: k_fwd_last<7, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 260: k_fwd_last<8, 4><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 291: k_fwd_last<9, 3><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 322: k_fwd_last<10, 2><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 353: k_fwd_last<11, 1><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 384: k_fwd_last<12, 0><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 230: k_fwd_last<7, 6><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 261: k_fwd_last<8, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 292: k_fwd_last<9, 4><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 323: k_fwd_last<10, 3><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 354: k_fwd_last<11, 2><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 385: k_fwd_last<12, 1><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 416: k_fwd_last<13, 0><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 231: k_fwd_last<7, 7><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 262: k_fwd_last<8, 6><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 293: k_fwd_last<9, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 324: k_fwd_last<10, 4><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 355: k_fwd_last<11, 3><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 386: k_fwd_last<12, 2><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 417: k_fwd_last<13, 1><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
+        case 448: k_fwd_last<14, 0><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, tw, jobs, g.zstride); break;
         default: return cudaErrorInvalidConfiguration;
     }
     return cudaGetLastError();

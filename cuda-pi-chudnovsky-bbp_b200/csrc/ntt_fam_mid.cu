@@ -8,24 +8,24 @@ namespace b2m {
 
 cudaError_t launch_fwd_mid(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw, const ProdJob* jobs, unsigned njobs, int operand) {
     switch (logr * 32 + g.logc) {
-        case 229: k_fwd_mid<7, 5><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 260: k_fwd_mid<8, 4><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 291: k_fwd_mid<9, 3><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 322: k_fwd_mid<10, 2><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 353: k_fwd_mid<11, 1><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 384: k_fwd_mid<12, 0><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 230: k_fwd_mid<7, 6><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 261: k_fwd_mid<8, 5><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 292: k_fwd_mid<9, 4><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 323: k_fwd_mid<10, 3><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 354: k_fwd_mid<11, 2><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 385: k_fwd_mid<12, 1><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 231: k_fwd_mid<7, 7><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 262: k_fwd_mid<8, 6><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 293: k_fwd_mid<9, 5><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 324: k_fwd_mid<10, 4><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 355: k_fwd_mid<11, 3><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
-        case 386: k_fwd_mid<12, 2><<<dim3(g.grid, njobs), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand); break;
+        case 229: k_fwd_mid<7, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 260: k_fwd_mid<8, 4><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 291: k_fwd_mid<9, 3><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 322: k_fwd_mid<10, 2><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 353: k_fwd_mid<11, 1><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 384: k_fwd_mid<12, 0><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 230: k_fwd_mid<7, 6><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 261: k_fwd_mid<8, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 292: k_fwd_mid<9, 4><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 323: k_fwd_mid<10, 3><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 354: k_fwd_mid<11, 2><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 385: k_fwd_mid<12, 1><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 231: k_fwd_mid<7, 7><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 262: k_fwd_mid<8, 6><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 293: k_fwd_mid<9, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 324: k_fwd_mid<10, 4><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 355: k_fwd_mid<11, 3><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
+        case 386: k_fwd_mid<12, 2><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tfwd, jobs, operand, g.zstride); break;
         default: return cudaErrorInvalidConfiguration;
     }
     return cudaGetLastError();

@@ -135,11 +135,12 @@ k_fwd_first(const u32* __restrict__ limbs, u64 ndig, u64* __restrict__ out, int 
 template <int LOGR, int LOGC>
 __global__ void B2M_PASS_BOUNDS((Tile<LOGR, LOGC, MAP_COL>::T))
 k_fwd_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const u64* __restrict__ ttab,
-          const ProdJob* __restrict__ jobs, int operand) {
+          const ProdJob* __restrict__ jobs, int operand, u64 zstride) {
     using TL = Tile<LOGR, LOGC, MAP_COL>;
     using G = ColPass<TL>;
     extern __shared__ u64 sm[];
     if (jobs) buf = operand ? jobs[blockIdx.y].bufB : jobs[blockIdx.y].bufA;
+    buf += blockIdx.z * zstride;  // sub-transform of a radix-3 plan
     const G gp(logS, logM);
 #pragma unroll
     for (int k = 0; k < G::PER; ++k) sm[gp.sa0 + G::soff(k)] = buf[gp.gi0 + k * gp.gstep];
@@ -166,11 +167,12 @@ k_fwd_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const u64* _
 template <int LOGR, int LOGC>
 __global__ void B2M_PASS_BOUNDS((Tile<LOGR, LOGC, MAP_COL>::T))
 k_inv_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const u64* __restrict__ ttab,
-          const ProdJob* __restrict__ jobs) {
+          const ProdJob* __restrict__ jobs, u64 zstride) {
     using TL = Tile<LOGR, LOGC, MAP_COL>;
     using G = ColPass<TL>;
     extern __shared__ u64 sm[];
     if (jobs) buf = jobs[blockIdx.y].bufB;
+    buf += blockIdx.z * zstride;
     const G gp(logS, logM);
     if (ttab) {
 #pragma unroll
@@ -195,11 +197,12 @@ k_inv_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const u64* _
 // sub-problem, so the CTA's tile is one contiguous range of R*C elements).
 template <int LOGR, int LOGC>
 __global__ void B2M_PASS_BOUNDS((Tile<LOGR, LOGC, MAP_ROW>::T))
-k_fwd_last(u64* __restrict__ buf, RootTables tw, const ProdJob* __restrict__ jobs) {
+k_fwd_last(u64* __restrict__ buf, RootTables tw, const ProdJob* __restrict__ jobs, u64 zstride) {
     using TL = Tile<LOGR, LOGC, MAP_ROW>;
     using G = RowPass<TL>;
     extern __shared__ u64 sm[];
     if (jobs) buf = jobs[blockIdx.y].bufA;
+    buf += blockIdx.z * zstride;
     const G gp;
     u64* base = buf + ((u64)blockIdx.x << (LOGR + LOGC)) + threadIdx.x;
 #pragma unroll
@@ -215,7 +218,7 @@ k_fwd_last(u64* __restrict__ buf, RootTables tw, const ProdJob* __restrict__ job
 template <int LOGR, int LOGC>
 __global__ void B2M_PASS_BOUNDS((Tile<LOGR, LOGC, MAP_ROW>::T))
 k_fused_last(u64* __restrict__ bbuf, const u64* __restrict__ aspec, u64 ninv, RootTables tw,
-             const ProdJob* __restrict__ jobs) {
+             const ProdJob* __restrict__ jobs, u64 zstride) {
     using TL = Tile<LOGR, LOGC, MAP_ROW>;
     using G = RowPass<TL>;
     extern __shared__ u64 sm[];
@@ -223,6 +226,8 @@ k_fused_last(u64* __restrict__ bbuf, const u64* __restrict__ aspec, u64 ninv, Ro
         bbuf = jobs[blockIdx.y].bufB;
         aspec = jobs[blockIdx.y].bufA;
     }
+    bbuf += blockIdx.z * zstride;
+    aspec += blockIdx.z * zstride;
     const G gp;
     const u64 off = ((u64)blockIdx.x << (LOGR + LOGC)) + threadIdx.x;
     u64* base = bbuf + off;

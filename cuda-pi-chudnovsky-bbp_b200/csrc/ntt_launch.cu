@@ -189,9 +189,39 @@ void twtable_free_all(Context* c) {
     c->twt.clear();
 }
 
-uint64_t carry_scratch_bytes(int logn) {
-    const uint64_t chunks = logn >= 12 ? (1ull << logn) / CARRY_CHUNK : 1;
+uint64_t carry_scratch_bytes(int logn) { return carry_scratch_bytes_n(1ull << logn); }
+
+uint64_t carry_scratch_bytes_n(uint64_t points) {
+    const uint64_t chunks = points >= CARRY_CHUNK ? points / CARRY_CHUNK : 1;
     return chunks * sizeof(LookbackSlot) + 256;
+}
+
+uint64_t workspace_bytes_plan(const Plan& p) {
+    if (p.npass == 0) return 256;
+    const uint64_t n = plan_points(p);
+    return 2 * 8 * n + carry_scratch_bytes_n(n);
+}
+
+void choose_length(uint64_t digits, int* logn, int* three) {
+    int l = 2;
+    while ((1ull << l) < digits) ++l;
+    if (l - 2 >= RADIX3_MIN_LOG && (3ull << (l - 2)) >= digits) {
+        *logn = l - 2;
+        *three = 1;
+    } else {
+        *logn = l;
+        *three = 0;
+    }
+}
+
+// Pass k's geometry; radix-3 plans run it over the three sub-transforms.
+static PassGeo geo(const Plan& p, int k) {
+    PassGeo g = pass_geo(p, k);
+    if (p.three) {
+        g.zdim = 3;
+        g.zstride = 1ull << p.logn;
+    }
+    return g;
 }
 
 uint64_t workspace_bytes_for(int logn) {
@@ -209,29 +239,39 @@ cudaError_t configure_kernels() {
     return e;
 }
 
-int plan_launches(const Plan& p) { return p.npass == 0 ? 1 : 3 * p.npass; }
+int plan_launches(const Plan& p) { return p.npass == 0 ? 1 : 3 * p.npass + (p.three ? 3 : 0); }
 
 static cudaError_t launch_forward(const u32* limbs, uint64_t nlimbs, u64* buf, const Plan& p,
                                   const RootTables& tw, bool fused, const u64* aspec, u64 ninv,
                                   cudaStream_t s, Tracer* tr) {
-    if (tr) tr->mark(s, B2M_K_FWD_FIRST, p.logr[0]);
-    cudaError_t e = launch_fwd_first(p.logr[0], pass_geo(p, 0), s, limbs, 2 * nlimbs, buf, tw);
-    for (int k = 1; e == cudaSuccess && k + 1 < p.npass; ++k) {
+    cudaError_t e;
+    int k0 = 0;
+    if (p.three) {
+        // radix-3 step from the digits, then the sub-transforms from pass 0
+        if (tr) tr->mark(s, B2M_K_R3_FWD, 0);
+        e = launch_r3_fwd(s, limbs, 2 * nlimbs, buf, p.logn, tw);
+    } else {
+        if (tr) tr->mark(s, B2M_K_FWD_FIRST, p.logr[0]);
+        e = launch_fwd_first(p.logr[0], geo(p, 0), s, limbs, 2 * nlimbs, buf, tw);
+        k0 = 1;
+    }
+    for (int k = k0; e == cudaSuccess && k + 1 < p.npass; ++k) {
         if (tr) tr->mark(s, B2M_K_FWD_MID, p.logr[k]);
-        e = launch_fwd_mid(p.logr[k], pass_geo(p, k), s, buf, tw);
+        e = launch_fwd_mid(p.logr[k], geo(p, k), s, buf, tw);
     }
     if (e != cudaSuccess) return e;
     const int last = p.npass - 1;
     if (tr) tr->mark(s, fused ? B2M_K_FUSED_LAST : B2M_K_FWD_LAST, p.logr[last]);
-    return fused ? launch_fused_last(p.logr[last], pass_geo(p, last), s, buf, aspec, ninv, tw)
-                 : launch_fwd_last(p.logr[last], pass_geo(p, last), s, buf, tw);
+    return fused ? launch_fused_last(p.logr[last], geo(p, last), s, buf, aspec, ninv, tw)
+                 : launch_fwd_last(p.logr[last], geo(p, last), s, buf, tw);
 }
 
 cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb, u32* out, uint64_t* out_len,
                            void* ws, const Plan& p, const RootTables& tw, u32* err, cudaStream_t s, Tracer* tr,
                            cudaEvent_t b_ready) {
     const int logn = p.logn;
-    const u64 ninv = gl_inv(1ull << logn);
+    const uint64_t n = plan_points(p);
+    const u64 ninv = gl_inv(n);
     const u64 nout = na + nb;
     if (p.npass == 0) {
         PassGeo g{};
@@ -250,7 +290,6 @@ cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb,
         if (tr) tr->end(s);
         return e;
     }
-    const uint64_t n = 1ull << logn;
     u64* bufA = static_cast<u64*>(ws);
     u64* bufB = bufA + n;
     unsigned char* scratch = reinterpret_cast<unsigned char*>(bufB + n);
@@ -258,7 +297,7 @@ cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb,
     LookbackSlot* slots = reinterpret_cast<LookbackSlot*>(scratch);
     u32* ticket = reinterpret_cast<u32*>(scratch + nchunks * sizeof(LookbackSlot));
     unsigned long long* len_tmp = reinterpret_cast<unsigned long long*>(ticket + 2);
-    cudaError_t e = cudaMemsetAsync(scratch, 0, carry_scratch_bytes(logn), s);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, carry_scratch_bytes_n(n), s);
     if (e != cudaSuccess) return e;
     unsigned long long* ol = out_len ? reinterpret_cast<unsigned long long*>(out_len) : len_tmp;
     if (out_len && (e = cudaMemsetAsync(out_len, 0, sizeof(uint64_t), s)) != cudaSuccess) return e;
@@ -268,7 +307,11 @@ cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb,
     if ((e = launch_forward(b, nb, bufB, p, tw, true, bufA, ninv, s, tr)) != cudaSuccess) return e;
     for (int k = p.npass - 2; k >= 0; --k) {
         if (tr) tr->mark(s, B2M_K_INV_MID, p.logr[k]);
-        if ((e = launch_inv_mid(p.logr[k], pass_geo(p, k), s, bufB, tw)) != cudaSuccess) return e;
+        if ((e = launch_inv_mid(p.logr[k], geo(p, k), s, bufB, tw)) != cudaSuccess) return e;
+    }
+    if (p.three) {
+        if (tr) tr->mark(s, B2M_K_R3_INV, 0);
+        if ((e = launch_r3_inv(s, bufB, logn, tw)) != cudaSuccess) return e;
     }
     if (tr) tr->mark(s, B2M_K_CARRY, 0);
     e = launch_carry((unsigned)nchunks, s, bufB, out, nout, slots, ticket, ol, err);
@@ -279,7 +322,7 @@ cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb,
 cudaError_t launch_bucket(const Plan& p, const ProdJob* jobs, unsigned njobs, const RootTables& tw, u32* err,
                           cudaStream_t s) {
     const int logn = p.logn;
-    const u64 ninv = gl_inv(1ull << logn);
+    const u64 ninv = gl_inv(plan_points(p));
     if (p.npass == 0) {
         PassGeo g{};
         const int T = logn >= 4 ? (1 << (logn - 4)) : 1;
@@ -291,18 +334,25 @@ cudaError_t launch_bucket(const Plan& p, const ProdJob* jobs, unsigned njobs, co
     }
     cudaError_t e = cudaSuccess;
     for (int op = 0; op < 2 && e == cudaSuccess; ++op) {
-        e = launch_fwd_first(p.logr[0], pass_geo(p, 0), s, nullptr, 0, nullptr, tw, jobs, njobs, op);
-        for (int k = 1; e == cudaSuccess && k + 1 < p.npass; ++k)
-            e = launch_fwd_mid(p.logr[k], pass_geo(p, k), s, nullptr, tw, jobs, njobs, op);
+        int k0 = 0;
+        if (p.three) {
+            e = launch_r3_fwd(s, nullptr, 0, nullptr, logn, tw, jobs, njobs, op);
+        } else {
+            e = launch_fwd_first(p.logr[0], geo(p, 0), s, nullptr, 0, nullptr, tw, jobs, njobs, op);
+            k0 = 1;
+        }
+        for (int k = k0; e == cudaSuccess && k + 1 < p.npass; ++k)
+            e = launch_fwd_mid(p.logr[k], geo(p, k), s, nullptr, tw, jobs, njobs, op);
         if (e != cudaSuccess) break;
         const int last = p.npass - 1;
-        e = op == 0 ? launch_fwd_last(p.logr[last], pass_geo(p, last), s, nullptr, tw, jobs, njobs)
-                    : launch_fused_last(p.logr[last], pass_geo(p, last), s, nullptr, nullptr, ninv, tw, jobs, njobs);
+        e = op == 0 ? launch_fwd_last(p.logr[last], geo(p, last), s, nullptr, tw, jobs, njobs)
+                    : launch_fused_last(p.logr[last], geo(p, last), s, nullptr, nullptr, ninv, tw, jobs, njobs);
     }
     for (int k = p.npass - 2; e == cudaSuccess && k >= 0; --k)
-        e = launch_inv_mid(p.logr[k], pass_geo(p, k), s, nullptr, tw, jobs, njobs);
+        e = launch_inv_mid(p.logr[k], geo(p, k), s, nullptr, tw, jobs, njobs);
+    if (e == cudaSuccess && p.three) e = launch_r3_inv(s, nullptr, logn, tw, jobs, njobs);
     if (e != cudaSuccess) return e;
-    const unsigned nchunks = (unsigned)((1ull << logn) / CARRY_CHUNK);
+    const unsigned nchunks = (unsigned)(plan_points(p) / CARRY_CHUNK);
     return launch_carry(nchunks, s, nullptr, nullptr, 0, nullptr, nullptr, nullptr, err, jobs, njobs);
 }
 

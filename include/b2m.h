@@ -75,7 +75,8 @@ const char* b2m_strerror(b2m_status status);
 /* Detail of the last failure on the calling thread ("" if none). */
 const char* b2m_last_error(void);
 
-/* Replaces ntt_length (include/ntt.h:47-50): next power of two >= 2na + 2nb. */
+/* Replaces ntt_length (include/ntt.h:47-50): next power of two >= 2na + 2nb.
+ * (The products may run on 3 * 2^k points instead; b2m_plan_describe tells.) */
 uint64_t b2m_ntt_length(uint64_t na, uint64_t nb);
 
 /* Device workspace in bytes that one product of na x nb limbs needs. */
@@ -339,7 +340,9 @@ enum {
     B2M_K_FUSED_LAST = 4,  /* operand B's last forward pass + pointwise + first inverse pass */
     B2M_K_INV_MID = 5,     /* an inverse pass (pass 1 yields the coefficients) */
     B2M_K_CARRY = 6,       /* decoupled-lookback carry into u32 limbs */
-    B2M_K_SMALL = 7        /* whole product in one CTA (transform length <= 2^13) */
+    B2M_K_SMALL = 7,       /* whole product in one CTA (transform length <= 2^13) */
+    B2M_K_R3_FWD = 8,      /* radix-3 step of a 3 * 2^k-point transform (digits in) */
+    B2M_K_R3_INV = 9       /* inverse radix-3 step (coefficients out, natural order) */
 };
 
 typedef struct b2m_plan_desc {
@@ -348,10 +351,14 @@ typedef struct b2m_plan_desc {
     uint32_t logr[3];       /* radix exponent of each pass */
     uint32_t logc[3];       /* columns per CTA (log2) of each pass */
     uint32_t launches;      /* kernels launched per product */
+    uint32_t three;         /* 1: 3 * 2^ntt_log2 points (a radix-3 step around three
+                               2^ntt_log2-point transforms with this pass plan) */
 } b2m_plan_desc;
 
 /* Describes the transform plan the library uses for an na x nb product (no
- * reference counterpart: the reference always runs radix-2 stages). */
+ * reference counterpart: the reference always runs radix-2 stages of
+ * next_pow2(2na + 2nb) points; this library uses 3 * 2^k points instead when
+ * that is fewer and k >= 14). */
 b2m_status b2m_plan_describe(uint64_t na, uint64_t nb, b2m_plan_desc* desc);
 
 /* One timed candidate of b2m_autotune. */
