@@ -199,9 +199,9 @@ _sig("b2m_autotune", ctypes.c_int, [_u64, _u64, ctypes.c_void_p, ctypes.POINTER(
 def autotune(na: int, nb: int, stream: int = 0) -> list[dict]:
     """Times every candidate plan for an na x nb product and keeps the
     fastest for that transform length (b2m_autotune). Returns the timings."""
-    out = (TuneEntry * 64)()
+    out = (TuneEntry * 512)()
     n = ctypes.c_uint32(0)
-    check(lib.b2m_autotune(na, nb, stream or None, out, 64, ctypes.byref(n)), "b2m_autotune")
+    check(lib.b2m_autotune(na, nb, stream or None, out, 512, ctypes.byref(n)), "b2m_autotune")
     res = []
     for e in out[: n.value]:
         k = max(e.plan.npass, 1)

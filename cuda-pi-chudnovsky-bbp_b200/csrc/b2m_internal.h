@@ -144,7 +144,7 @@ PassGeo pass_geo(const Plan& p, int k);
 // never while `s` is capturing, skipped if the budget is short); pass_geo
 // only looks them up, so launch paths that must not allocate still use
 // tables that exist.
-constexpr int TWT_MIN_LOGM = 20;
+constexpr int TWT_MIN_LOGM = 12;
 struct Context;
 cudaError_t twtable_ensure(Context* c, const Plan& p, cudaStream_t s);
 void twtable_free_all(Context* c);

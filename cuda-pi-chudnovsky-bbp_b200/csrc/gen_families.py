@@ -17,7 +17,7 @@ TILES = (12, 13, 14)
 
 
 def combos(rmax):
-    return [(r, t - r) for t in TILES for r in range(7, min(rmax, t) + 1)]
+    return [(r, t - r) for t in TILES for r in range(6, min(rmax, t) + 1)]
 
 
 COL = combos(12)   # first, middle and non-last inverse passes (radix <= 2^12)

@@ -8,12 +8,14 @@ namespace b2m {
 
 cudaError_t launch_fused_last(int logr, const PassGeo& g, cudaStream_t s, u64* bbuf, const u64* aspec, u64 ninv, const RootTables& tw, const ProdJob* jobs, unsigned njobs) {
     switch (logr * 32 + g.logc) {
+        case 198: k_fused_last<6, 6><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
         case 229: k_fused_last<7, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
         case 260: k_fused_last<8, 4><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
         case 291: k_fused_last<9, 3><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
         case 322: k_fused_last<10, 2><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
         case 353: k_fused_last<11, 1><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
         case 384: k_fused_last<12, 0><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 199: k_fused_last<6, 7><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
         case 230: k_fused_last<7, 6><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
         case 261: k_fused_last<8, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
         case 292: k_fused_last<9, 4><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
@@ -21,6 +23,7 @@ cudaError_t launch_fused_last(int logr, const PassGeo& g, cudaStream_t s, u64* b
         case 354: k_fused_last<11, 2><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
         case 385: k_fused_last<12, 1><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
         case 416: k_fused_last<13, 0><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
+        case 200: k_fused_last<6, 8><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
         case 231: k_fused_last<7, 7><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
         case 262: k_fused_last<8, 6><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
         case 293: k_fused_last<9, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(bbuf, aspec, ninv, tw, jobs, g.zstride); break;
@@ -36,12 +39,14 @@ cudaError_t launch_fused_last(int logr, const PassGeo& g, cudaStream_t s, u64* b
 
 cudaError_t configure_fused() {
     cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<6, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<7, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<9, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<10, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<11, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<12, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<6, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<7, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<8, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<9, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
@@ -49,6 +54,7 @@ cudaError_t configure_fused() {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<11, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<12, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<13, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<6, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<7, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<8, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused_last<9, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);

@@ -8,18 +8,21 @@ namespace b2m {
 
 cudaError_t launch_inv_mid(int logr, const PassGeo& g, cudaStream_t s, u64* buf, const RootTables& tw, const ProdJob* jobs, unsigned njobs) {
     switch (logr * 32 + g.logc) {
+        case 198: k_inv_mid<6, 6><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
         case 229: k_inv_mid<7, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
         case 260: k_inv_mid<8, 4><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
         case 291: k_inv_mid<9, 3><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
         case 322: k_inv_mid<10, 2><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
         case 353: k_inv_mid<11, 1><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
         case 384: k_inv_mid<12, 0><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 199: k_inv_mid<6, 7><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
         case 230: k_inv_mid<7, 6><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
         case 261: k_inv_mid<8, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
         case 292: k_inv_mid<9, 4><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
         case 323: k_inv_mid<10, 3><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
         case 354: k_inv_mid<11, 2><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
         case 385: k_inv_mid<12, 1><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
+        case 200: k_inv_mid<6, 8><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
         case 231: k_inv_mid<7, 7><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
         case 262: k_inv_mid<8, 6><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
         case 293: k_inv_mid<9, 5><<<dim3(g.grid, njobs, g.zdim), g.block, g.smem, s>>>(buf, g.logs, g.logm, tw, g.tinv, jobs, g.zstride); break;
@@ -33,18 +36,21 @@ cudaError_t launch_inv_mid(int logr, const PassGeo& g, cudaStream_t s, u64* buf,
 
 cudaError_t configure_inv() {
     cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<6, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<7, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<9, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<10, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<11, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<12, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<6, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<7, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<8, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<9, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<10, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<11, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<12, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<6, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<7, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<8, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_inv_mid<9, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);

@@ -27,11 +27,48 @@
 
 namespace b2m {
 
-Plan make_plan(int logn) { return make_plan_custom(logn, -1, -1); }
+// Default plans for 2^14..2^27 points: the autotuner's fastest candidate on
+// a B200 for a square product of each length (uniform random limbs, median
+// of three). Small lengths favour 2^12-element tiles (more CTAs for little
+// work); 2^20..2^24 two passes with a 2^12..2^13 contiguous last pass;
+// 2^25 and up three passes of 2^12-element tiles, whose extra HBM sweep
+// costs less than the latency one 2^14-element CTA per SM leaves exposed.
+namespace {
+struct DefaultPlan {
+    int npass, r0, r1, r2, tile;
+};
+constexpr int DEFAULT_MIN_LOGN = 14, DEFAULT_MAX_LOGN = 27;
+constexpr DefaultPlan kDefaultPlans[DEFAULT_MAX_LOGN - DEFAULT_MIN_LOGN + 1] = {
+    {2, 8, 6, 0, 12},    // 2^14
+    {2, 7, 8, 0, 12},    // 2^15
+    {2, 8, 8, 0, 12},    // 2^16
+    {2, 9, 8, 0, 12},    // 2^17
+    {2, 6, 12, 0, 12},   // 2^18
+    {2, 7, 12, 0, 12},   // 2^19
+    {2, 8, 12, 0, 13},   // 2^20
+    {2, 9, 12, 0, 13},   // 2^21
+    {2, 10, 12, 0, 12},  // 2^22
+    {2, 10, 13, 0, 13},  // 2^23
+    {2, 11, 13, 0, 13},  // 2^24
+    {3, 9, 8, 8, 12},    // 2^25
+    {3, 9, 9, 8, 12},    // 2^26
+    {3, 9, 7, 11, 12},   // 2^27
+};
+}  // namespace
 
-// r0 < 0 / tile < 0 pick the defaults: two passes up to 2^26, the first pass
-// keeping at least 4 columns (32-byte rows) in a 2^14-element tile and the
-// last (contiguous) pass taking up to 2^14; three passes above.
+Plan make_plan(int logn) {
+    if (logn <= SMALL_MAX_LOGN) return make_plan_split(logn, nullptr, 0, -1);
+    if (logn >= DEFAULT_MIN_LOGN && logn <= DEFAULT_MAX_LOGN) {
+        const DefaultPlan& d = kDefaultPlans[logn - DEFAULT_MIN_LOGN];
+        const int r[3] = {d.r0, d.r1, d.r2};
+        return make_plan_split(logn, r, d.npass, d.tile);
+    }
+    return make_plan_custom(logn, -1, 12);
+}
+
+// r0 < 0 picks a default split: two passes up to 2^26, the first radix at
+// most 2^12 (a first pass keeps >= 4 columns, 32-byte rows, in its tile) and
+// the last (contiguous) pass up to 2^14; three near-equal passes above.
 Plan make_plan_custom(int logn, int r0, int tile) {
     if (logn <= SMALL_MAX_LOGN) return make_plan_split(logn, nullptr, 0, tile);
     int r[3];
@@ -70,18 +107,18 @@ Plan make_plan_split(int logn, const int* r, int npass, int tile) {
 }
 
 // Plans the autotuners time: every two-pass split with a first radix of
-// 2^7..2^12 and a last of 2^7..2^14, and the balanced three-pass splits (each
-// radix within one of logn / 3), each at tiles of 2^12, 2^13 and 2^14
-// elements where the radices fit.
+// 2^6..2^12 and a last of 2^6..2^14, and from 2^21 points every three-pass
+// split with radices 2^6..2^12 (the last up to 2^14), each at tiles of 2^12,
+// 2^13 and 2^14 elements where the radices fit.
 std::vector<Plan> plan_candidates(int logn) {
     std::vector<Plan> v;
     if (logn <= SMALL_MAX_LOGN) {
         v.push_back(make_plan(logn));
         return v;
     }
-    for (int r0 = 7; r0 <= 12; ++r0) {
+    for (int r0 = 6; r0 <= 12; ++r0) {
         const int r1 = logn - r0;
-        if (r1 < 7 || r1 > 14) continue;
+        if (r1 < 6 || r1 > 14) continue;
         for (int tile = 12; tile <= 14; ++tile) {
             if (r0 > tile || r1 > tile) continue;
             const int r[2] = {r0, r1};
@@ -89,11 +126,10 @@ std::vector<Plan> plan_candidates(int logn) {
         }
     }
     if (logn >= 21) {
-        const int t = logn / 3;
-        for (int r0 = std::max(7, t - 1); r0 <= std::min(12, t + 1); ++r0)
-            for (int r1 = std::max(7, t - 1); r1 <= std::min(12, t + 1); ++r1) {
+        for (int r0 = 6; r0 <= 12; ++r0)
+            for (int r1 = 6; r1 <= 12; ++r1) {
                 const int r2 = logn - r0 - r1;
-                if (r2 < 7 || r2 > 14) continue;
+                if (r2 < 6 || r2 > 14) continue;
                 for (int tile = 12; tile <= 14; ++tile) {
                     if (r0 > tile || r1 > tile || r2 > tile) continue;
                     const int r[3] = {r0, r1, r2};
