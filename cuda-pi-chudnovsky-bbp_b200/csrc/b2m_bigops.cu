@@ -606,8 +606,12 @@ constexpr int DC_LEAF_J = 2;     // leaves: values below P_2^2 = 10^72
 constexpr int DC_LEAF_LIMBS = 8;  // 10^72 < 2^240
 constexpr int DC_LEAF_GROUPS = 8;
 
+// Job i multiplies a + i*sa by b + i*sb. With `spec` (b shared, sb = 0, its
+// spectrum already in spec), b becomes every job's first operand with bufA =
+// spec, and the workspace holds only bufB and the carry scratch.
 __global__ void k_dc_jobs(const u32* a, u64 sa, u64 na, const u32* b, u64 sb, u64 nb, u32* out, u64 so,
-                          unsigned long long* lens, ProdJob* jobs, u64 njobs, unsigned char* ws, u64 wss, u64 npts) {
+                          unsigned long long* lens, ProdJob* jobs, u64 njobs, unsigned char* ws, u64 wss, u64 npts,
+                          u64* spec) {
     const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= njobs) return;
     ProdJob J{};
@@ -615,17 +619,40 @@ __global__ void k_dc_jobs(const u32* a, u64 sa, u64 na, const u32* b, u64 sb, u6
     J.na = na;
     J.b = b + i * sb;
     J.nb = nb;
+    if (spec) {
+        J.a = b;
+        J.na = nb;
+        J.b = a + i * sa;
+        J.nb = na;
+    }
     J.out = out + i * so;
     J.out_len = lens + i;
     if (wss) {
         const u64 n = npts;
         unsigned char* w = ws + i * wss;
-        J.bufA = reinterpret_cast<u64*>(w);
-        J.bufB = J.bufA + n;
-        J.slots = reinterpret_cast<LookbackSlot*>(w + 16 * n);
-        J.ticket = reinterpret_cast<u32*>(w + 16 * n + (n / CARRY_CHUNK) * sizeof(LookbackSlot));
+        unsigned char* scratch;
+        if (spec) {
+            J.bufA = spec;
+            J.bufB = reinterpret_cast<u64*>(w);
+            scratch = w + 8 * n;
+        } else {
+            J.bufA = reinterpret_cast<u64*>(w);
+            J.bufB = J.bufA + n;
+            scratch = w + 16 * n;
+        }
+        J.slots = reinterpret_cast<LookbackSlot*>(scratch);
+        J.ticket = reinterpret_cast<u32*>(scratch + (n / CARRY_CHUNK) * sizeof(LookbackSlot));
     }
     jobs[i] = J;
+}
+
+// The one-job table that transforms b into spec.
+__global__ void k_dc_spec_job(const u32* b, u64 nb, u64* spec, ProdJob* job) {
+    ProdJob J{};
+    J.a = b;
+    J.na = nb;
+    J.bufA = spec;
+    *job = J;
 }
 
 __global__ void k_dc_zero_ws(const ProdJob* __restrict__ jobs, u64 njobs, u64 scratch_words) {
@@ -637,7 +664,9 @@ __global__ void k_dc_zero_ws(const ProdJob* __restrict__ jobs, u64 njobs, u64 sc
 }
 
 // out_i = a_i * b_i for m products of na x nb limbs (strides sa, sb, so; sb = 0
-// shares one b), as size-bucketed launches of the batch path.
+// shares one b), as size-bucketed launches of the batch path. A shared b is
+// transformed once and its spectrum read by every product (two transforms a
+// product instead of three).
 void batched_mul(Scope& S, const u32* a, uint64_t sa, uint64_t na, const u32* b, uint64_t sb, uint64_t nb, u32* out,
                  uint64_t so, uint64_t m) {
     if (m == 0) return;
@@ -648,7 +677,17 @@ void batched_mul(Scope& S, const u32* a, uint64_t sa, uint64_t na, const u32* b,
     const Plan p = product_plan(c, na, nb);
     ck(twtable_ensure(c, p, S.s()), "twiddle table");
     const uint64_t npts = plan_points(p);
-    const uint64_t wss = p.npass ? ((workspace_bytes_plan(p) + 255) & ~255ull) : 0;
+    u64* spec = nullptr;
+    if (sb == 0 && m > 1 && p.npass > 0) {
+        spec = static_cast<u64*>(S.raw(8 * npts));
+        ProdJob* sj = static_cast<ProdJob*>(S.raw(sizeof(ProdJob)));
+        k_dc_spec_job<<<1, 1, 0, S.s()>>>(b, nb, spec, sj);
+        ck(cudaGetLastError(), "spectrum job");
+        ck(launch_bucket_spectrum(p, sj, 1, c->tw, S.s()), "shared spectrum");
+    }
+    const uint64_t wss = !p.npass ? 0
+                         : spec   ? ((8 * npts + carry_scratch_bytes_n(npts) + 255) & ~255ull)
+                                  : ((workspace_bytes_plan(p) + 255) & ~255ull);
     // at most 65535 jobs a launch, and at most ~1 GiB of transform workspace
     uint64_t chunk = 65535;
     if (wss) chunk = std::max<uint64_t>(1, std::min<uint64_t>(chunk, (1ull << 30) / wss));
@@ -658,10 +697,11 @@ void batched_mul(Scope& S, const u32* a, uint64_t sa, uint64_t na, const u32* b,
         unsigned long long* lens = static_cast<unsigned long long*>(S.raw(nj * 8));
         unsigned char* ws = wss ? static_cast<unsigned char*>(S.raw(nj * wss)) : nullptr;
         k_dc_jobs<<<(unsigned)((nj + 255) / 256), 256, 0, S.s()>>>(a + off * sa, sa, na, b + off * sb, sb, nb,
-                                                                  out + off * so, so, lens, jobs, nj, ws, wss, npts);
+                                                                  out + off * so, so, lens, jobs, nj, ws, wss, npts,
+                                                                  spec);
         if (wss) k_dc_zero_ws<<<(unsigned)nj, 256, 0, S.s()>>>(jobs, nj, carry_scratch_bytes_n(npts) / 8);
         ck(cudaGetLastError(), "job tables");
-        ck(launch_bucket(p, jobs, (unsigned)nj, c->tw, c->d_err, S.s()), "batched product");
+        ck(launch_bucket(p, jobs, (unsigned)nj, c->tw, c->d_err, S.s(), spec != nullptr), "batched product");
     }
 }
 
@@ -788,6 +828,45 @@ __global__ void k_dc_leaf(const u32* __restrict__ nodes, u64 stride, u64 m, char
     }
 }
 
+// k_dc_fix's steps for one node as grid-wide passes driven from the host:
+// for the top levels, whose few nodes have up to millions of limbs, one CTA
+// a node would leave the GPU idle. R = V - U over w limbs, then R += P with
+// q -= 1 while R is negative, then R -= P with q += 1 while R >= P; q and R
+// go to oq / orr (n limbs, zero-padded to sout). R, T: w limbs; Q: nq + 1.
+void fix_node_grid(Scope& S, const u32* V, uint64_t sin, const u32* U, uint64_t su, const u32* QE, uint64_t nq,
+                   DV Pj, DV R, DV T, DV Q, DV one, u32* oq, u32* orr, uint64_t sout) {
+    const uint64_t n = Pj.n;
+    ck(cudaMemsetAsync(Q.p, 0, 4 * (nq + 1), S.s()), "cudaMemsetAsync");
+    ck(cudaMemcpyAsync(Q.p, QE, 4 * nq, cudaMemcpyDeviceToDevice, S.s()), "D2D");
+    u32 neg = addsub(S, {const_cast<u32*>(V), sin}, {const_cast<u32*>(U), su}, R, true);
+    int it = 0;
+    while (neg && it < 64) {
+        if (addsub(S, R, Pj, R, false)) neg = 0;
+        addsub(S, Q, one, Q, true);
+        ++it;
+    }
+    while (it < 64) {
+        if (addsub(S, R, Pj, T, true)) break;
+        std::swap(R, T);
+        addsub(S, Q, one, Q, false);
+        ++it;
+    }
+    if (it >= 64) {
+        set_error("decimal conversion: a quotient correction did not converge");
+        throw Err{B2M_ERR_INTERNAL};
+    }
+    ck(cudaMemsetAsync(oq, 0, 4 * sout, S.s()), "cudaMemsetAsync");
+    ck(cudaMemsetAsync(orr, 0, 4 * sout, S.s()), "cudaMemsetAsync");
+    const uint64_t k = std::min(n, sout);
+    ck(cudaMemcpyAsync(oq, Q.p, 4 * std::min(k, nq + 1), cudaMemcpyDeviceToDevice, S.s()), "D2D");
+    ck(cudaMemcpyAsync(orr, R.p, 4 * std::min(k, R.n), cudaMemcpyDeviceToDevice, S.s()), "D2D");
+}
+
+// Levels with at most this many nodes, of at least DC_GRID_MIN_LIMBS limbs,
+// fix their nodes with grid-wide passes (fix_node_grid).
+constexpr uint64_t DC_GRID_MAX_NODES = 16;
+constexpr uint64_t DC_GRID_MIN_LIMBS = 1 << 15;
+
 // -1, 0, 1 as a <, ==, > b (trimmed).
 int cmp(Scope& S, DV a, DV b) {
     if (a.n != b.n) return a.n < b.n ? -1 : 1;
@@ -860,12 +939,22 @@ std::string to_decimal(Scope& S, DV X) {
         const uint64_t sout = j - 1 > DC_LEAF_J ? 2 * P[j - 1].n : DC_LEAF_LIMBS;
         DV out = S.vec(2 * m * sout);
         const uint64_t w = std::max(sin, su) + 1;
-        DV scr = S.vec(m * (2 * w + nq + 1));
-        unsigned threads = 32;
-        while (threads < 1024 && (uint64_t)threads * ADD_LPT < w) threads <<= 1;
-        k_dc_fix<<<(unsigned)m, threads, 0, S.s()>>>(in.p, sin, U.p, su, qe.p, nq, Pj.p, n, scr.p, w, out.p, sout,
-                                                     err);
-        ck(cudaGetLastError(), "k_dc_fix");
+        if (m <= DC_GRID_MAX_NODES && w >= DC_GRID_MIN_LIMBS) {
+            DV R = S.vec(w), T = S.vec(w), Q = S.vec(nq + 1);
+            DV one = S.vec(1);
+            static const u32 one_h = 1;
+            ck(cudaMemcpyAsync(one.p, &one_h, 4, cudaMemcpyHostToDevice, S.s()), "H2D");
+            for (uint64_t i = 0; i < m; ++i)
+                fix_node_grid(S, in.p + i * sin, sin, U.p + i * su, su, qe.p + i * nq, nq, Pj, R, T, Q, one,
+                              out.p + (2 * i) * sout, out.p + (2 * i + 1) * sout, sout);
+        } else {
+            DV scr = S.vec(m * (2 * w + nq + 1));
+            unsigned threads = 32;
+            while (threads < 1024 && (uint64_t)threads * ADD_LPT < w) threads <<= 1;
+            k_dc_fix<<<(unsigned)m, threads, 0, S.s()>>>(in.p, sin, U.p, su, qe.p, nq, Pj.p, n, scr.p, w, out.p,
+                                                         sout, err);
+            ck(cudaGetLastError(), "k_dc_fix");
+        }
         in = out;
         sin = sout;
         m *= 2;
@@ -923,6 +1012,51 @@ void put(Scope& S, DV v, uint32_t* dst, uint64_t cap, uint64_t* len) {
 }
 
 }  // namespace big
+
+// ---------------------------------------------------------------------------- launchers for other files
+namespace {
+__global__ void k_top_diff(const u32* __restrict__ a, const u32* __restrict__ b, u64 n, unsigned long long* out) {
+    unsigned long long t = 0;
+    for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (u64)gridDim.x * blockDim.x)
+        if (a[k] != b[k]) t = k + 1;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long o = __shfl_xor_sync(0xFFFFFFFFu, t, off);
+        t = o > t ? o : t;
+    }
+    if ((threadIdx.x & 31) == 0 && t) atomicMax(out, t);
+}
+}  // namespace
+
+uint64_t addsub_scratch_bytes(uint64_t n) {
+    const uint64_t nb = (n + big::AS_CH - 1) / big::AS_CH;
+    return ((nb * sizeof(GP) + 255) & ~255ull) + ((nb * 4 + 255) & ~255ull);
+}
+
+cudaError_t launch_addsub(const u32* a, uint64_t la, const u32* b, uint64_t lb, uint64_t n, int sub, u32* out,
+                          void* scratch, u32* flag, cudaStream_t s) {
+    if (n == 0) return cudaMemsetAsync(flag, 0, 4, s);
+    const uint64_t nb = (n + big::AS_CH - 1) / big::AS_CH;
+    GP* agg = static_cast<GP*>(scratch);
+    u32* cin = reinterpret_cast<u32*>(static_cast<unsigned char*>(scratch) + ((nb * sizeof(GP) + 255) & ~255ull));
+    big::k_as_reduce<<<(unsigned)nb, big::AS_T, 0, s>>>(a, la, b, lb, n, sub, agg);
+    big::k_as_scan<<<1, 1024, 0, s>>>(agg, nb, cin, flag);
+    big::k_as_apply<<<(unsigned)nb, big::AS_T, 0, s>>>(a, la, b, lb, n, sub, cin, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_top(const u32* a, uint64_t n, unsigned long long* out, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    big::k_top<<<big::grid_for(n), 256, 0, s>>>(a, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_top_diff(const u32* a, const u32* b, uint64_t n, unsigned long long* out, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    k_top_diff<<<big::grid_for(n), 256, 0, s>>>(a, b, n, out);
+    return cudaGetLastError();
+}
+
 }  // namespace b2m
 
 using namespace b2m;

@@ -120,11 +120,11 @@ __device__ __forceinline__ MergeProd merge_prod(const LevelView& L, const LevelV
         case 0:  // P' = PL * PR
             p = {val(0, l), ln(0, l), val(0, r), ln(0, r), Ln.limbs[0] + i * Ln.stride[0], Ln.len + i};
             break;
-        case 1:  // Q' = QL * QR
-            p = {val(1, l), ln(1, l), val(1, r), ln(1, r), Ln.limbs[1] + i * Ln.stride[1], Ln.len + Ln.m + i};
+        case 1:  // Q' = QR * QL (QR first: X shares its spectrum)
+            p = {val(1, r), ln(1, r), val(1, l), ln(1, l), Ln.limbs[1] + i * Ln.stride[1], Ln.len + Ln.m + i};
             break;
-        case 2:  // X = TL * QR
-            p = {val(2, l), ln(2, l), val(1, r), ln(1, r), S.x + i * S.sx, S.lx + i};
+        case 2:  // X = QR * TL
+            p = {val(1, r), ln(1, r), val(2, l), ln(2, l), S.x + i * S.sx, S.lx + i};
             break;
         default:  // Y = PL * TR
             p = {val(0, l), ln(0, l), val(2, r), ln(2, r), S.y + i * S.sy, S.ly + i};
@@ -179,9 +179,13 @@ __global__ void __launch_bounds__(SCHOOL_WARPS * 32) k_bs_school(LevelView L, Le
     }
 }
 
-// Job tables of one product kind for the NTT buckets.
+// Job tables of one product kind for the NTT buckets. With spec_ws, job i's
+// first operand is already transformed in the bufA of the partner product's
+// job i (its workspace at spec_ws + i * spec_stride), and this job's
+// workspace holds only bufB and the carry scratch.
 __global__ void k_bs_build_jobs(LevelView L, LevelView Ln, ScratchXY S, u64 m2, int kind, ProdJob* jobs,
-                                unsigned char* ntt_ws, u64 ws_stride, u64 npts) {
+                                unsigned char* ntt_ws, u64 ws_stride, u64 npts, unsigned char* spec_ws,
+                                u64 spec_stride) {
     const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m2) return;
     const MergeProd p = merge_prod(L, Ln, S, i, kind);
@@ -195,10 +199,18 @@ __global__ void k_bs_build_jobs(LevelView L, LevelView Ln, ScratchXY S, u64 m2, 
     if (ntt_ws) {
         const u64 n = npts;
         unsigned char* w = ntt_ws + i * ws_stride;
-        J.bufA = reinterpret_cast<u64*>(w);
-        J.bufB = J.bufA + n;
-        J.slots = reinterpret_cast<LookbackSlot*>(w + 16 * n);
-        J.ticket = reinterpret_cast<u32*>(w + 16 * n + (n / CARRY_CHUNK) * sizeof(LookbackSlot));
+        unsigned char* scratch;
+        if (spec_ws) {
+            J.bufA = reinterpret_cast<u64*>(spec_ws + i * spec_stride);
+            J.bufB = reinterpret_cast<u64*>(w);
+            scratch = w + 8 * n;
+        } else {
+            J.bufA = reinterpret_cast<u64*>(w);
+            J.bufB = J.bufA + n;
+            scratch = w + 16 * n;
+        }
+        J.slots = reinterpret_cast<LookbackSlot*>(scratch);
+        J.ticket = reinterpret_cast<u32*>(scratch + (n / CARRY_CHUNK) * sizeof(LookbackSlot));
     }
     jobs[i] = J;
 }
@@ -421,6 +433,98 @@ static int ceil_log2(uint64_t x) {
 }
 
 // One level: L (m nodes, max lengths mx) -> Ln.
+// k_bs_signed_add's operation as grid-wide passes driven from the host, for
+// levels of a few merges with up to millions of limbs (the top of the tree),
+// where one CTA a merge would leave the GPU idle. Reads each merge's lengths
+// and signs back, compares |X| and |Y| when it subtracts, and writes T's
+// magnitude, length and sign.
+constexpr uint64_t BS_GRID_MAX_MERGES = 8;
+constexpr uint64_t BS_GRID_MIN_LIMBS = 1 << 15;
+
+static cudaError_t signed_add_grid(Context* c, const ScratchXY& S, const int* sign_l, const LevelView& Ln,
+                                   uint64_t m2, uint64_t capT, cudaStream_t s) {
+    std::vector<u64> lx(m2), ly(m2);
+    std::vector<int> sg(2 * m2);
+    cudaError_t e = cudaMemcpyAsync(lx.data(), S.lx, 8 * m2, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ly.data(), S.ly, 8 * m2, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sg.data(), sign_l, sizeof(int) * 2 * m2, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    const uint64_t sb = addsub_scratch_bytes(capT) + 256;
+    if (!budget_reserve(c, sb)) return cudaErrorMemoryAllocation;
+    void* scratch = nullptr;
+    if ((e = cudaMallocAsync(&scratch, sb, s)) != cudaSuccess) {
+        budget_release(c, sb);
+        return e;
+    }
+    unsigned long long* word = reinterpret_cast<unsigned long long*>(static_cast<unsigned char*>(scratch) + sb - 256);
+    u32* flag = reinterpret_cast<u32*>(word + 1);
+    auto read_word = [&](unsigned long long* h) {
+        cudaError_t r = cudaMemcpyAsync(h, word, 8, cudaMemcpyDeviceToHost, s);
+        return r == cudaSuccess ? cudaStreamSynchronize(s) : r;
+    };
+    for (uint64_t i = 0; i < m2 && e == cudaSuccess; ++i) {
+        const u32* X = S.x + i * S.sx;
+        const u32* Y = S.y + i * S.sy;
+        uint64_t la = lx[i], lb = ly[i];
+        int sx = la ? sg[2 * i] : 0, sy = lb ? sg[2 * i + 1] : 0;
+        u32* out = Ln.limbs[2] + i * Ln.stride[2];
+        bool sub = false, swap = false, cancel = false;
+        int sres = 0;
+        if (sx == 0) {
+            sres = sy;
+            swap = true;
+            la = 0;
+        } else if (sy == 0) {
+            sres = sx;
+            lb = 0;
+        } else if (sx == sy) {
+            sres = sx;
+        } else {
+            sub = true;
+            int cmpv = 0;
+            if (la != lb) {
+                cmpv = la > lb ? 1 : -1;
+            } else {
+                unsigned long long d = 0;
+                if ((e = cudaMemsetAsync(word, 0, 8, s)) == cudaSuccess && (e = launch_top_diff(X, Y, la, word, s)) ==
+                    cudaSuccess)
+                    e = read_word(&d);
+                if (e == cudaSuccess && d) {
+                    u32 xv = 0, yv = 0;
+                    e = cudaMemcpyAsync(&xv, X + d - 1, 4, cudaMemcpyDeviceToHost, s);
+                    if (e == cudaSuccess) e = cudaMemcpyAsync(&yv, Y + d - 1, 4, cudaMemcpyDeviceToHost, s);
+                    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                    cmpv = xv > yv ? 1 : -1;
+                }
+            }
+            if (cmpv == 0) cancel = true;  // exact cancellation (or an error, reported below)
+            swap = cmpv < 0;
+            sres = swap ? sy : sx;
+        }
+        if (e != cudaSuccess) break;
+        unsigned long long top = 0;
+        if (!cancel) {
+            const u32* A = swap ? Y : X;  // the larger magnitude when subtracting
+            const u32* B = swap ? X : Y;
+            const uint64_t na = swap ? lb : la, nb = swap ? la : lb;
+            const uint64_t n = std::max(na, nb) + (sub ? 0 : 1);
+            e = launch_addsub(A, na, B, nb, n, sub ? 1 : 0, out, scratch, flag, s);
+            if (e == cudaSuccess) e = cudaMemsetAsync(word, 0, 8, s);
+            if (e == cudaSuccess) e = launch_top(out, n, word, s);
+            if (e == cudaSuccess) e = read_word(&top);
+        }
+        const u64 len = top;
+        const int sign = top ? sres : 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(Ln.len + 2 * Ln.m + i, &len, 8, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(Ln.sign + i, &sign, sizeof(int), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // len and sign are stack values
+    }
+    cudaFreeAsync(scratch, s);
+    budget_release(c, sb);
+    return e;
+}
+
 static cudaError_t merge_level(Context* c, const LevelView& L, const uint64_t mx[3], LevelView* Ln, void** mem_n,
                                uint64_t* bytes_n, uint64_t* products, cudaStream_t s) {
     const uint64_t m = L.m, m2 = m / 2, mn = m2 + (m & 1);
@@ -466,16 +570,51 @@ static cudaError_t merge_level(Context* c, const LevelView& L, const uint64_t mx
     }
     std::vector<void*> tmp;
     std::vector<uint64_t> tmpb;
-    for (int k = 0; k < 4 && m2 && e == cudaSuccess; ++k) {
-        if ((school_mask >> k) & 1) continue;
-        if (ceil_log2(2 * cap[k]) > MAX_LOGN) return cudaErrorInvalidValue;
+    for (int k = 0; k < 4; ++k)
+        if (!((school_mask >> k) & 1) && ceil_log2(2 * cap[k]) > MAX_LOGN) return cudaErrorInvalidValue;
+    auto kind_plan = [&](int k) {
         int logn = 0, three = 0;
         choose_length(2 * cap[k], &logn, &three);
         Plan p = plan_for(c, logn);
         p.three = three;
+        return p;
+    };
+    // Pairs that share a forward spectrum: Q = QR*QL then X = QR*TL (QR), and
+    // P = PL*PR then Y = PL*TR (PL). A shared pair runs both products under
+    // the longer of their plans, when its five transforms cost fewer points
+    // than the six of two separate products.
+    const int order[4] = {1, 2, 0, 3};
+    bool pair_share = false;
+    Plan pair_plan;
+    unsigned char* pair_ws = nullptr;
+    uint64_t pair_wss = 0;
+    for (int oi = 0; oi < 4 && m2 && e == cudaSuccess; ++oi) {
+        const int k = order[oi];
+        const bool second = (oi & 1) != 0;
+        if (!second) pair_share = false;
+        if ((school_mask >> k) & 1) continue;
+        Plan p = kind_plan(k);
+        bool use_spec = false;
+        if (!second) {
+            const int partner = order[oi + 1];
+            if (!((school_mask >> partner) & 1)) {
+                const Plan q = kind_plan(partner);
+                const uint64_t n1 = plan_points(p), n2 = plan_points(q), nmax = std::max(n1, n2);
+                if (5 * nmax < 3 * (n1 + n2)) {
+                    if (n2 > n1) p = q;
+                    pair_share = p.npass > 0;
+                }
+            }
+            pair_plan = p;
+        } else if (pair_share) {
+            p = pair_plan;
+            use_spec = true;
+        }
         const uint64_t npts = plan_points(p);
         if ((e = twtable_ensure(c, p, s)) != cudaSuccess) break;
-        const uint64_t wss = p.npass ? al(workspace_bytes_plan(p)) : 0;
+        const uint64_t wss = !p.npass ? 0
+                             : use_spec ? al(8 * npts + carry_scratch_bytes_n(npts))
+                                        : al(workspace_bytes_plan(p));
         const uint64_t tb = al(m2 * sizeof(ProdJob)) + m2 * wss;
         void* t = nullptr;
         if (!budget_reserve(c, tb)) {
@@ -490,7 +629,8 @@ static cudaError_t merge_level(Context* c, const LevelView& L, const uint64_t mx
         tmpb.push_back(tb);
         ProdJob* jobs = static_cast<ProdJob*>(t);
         unsigned char* ws = wss ? static_cast<unsigned char*>(t) + al(m2 * sizeof(ProdJob)) : nullptr;
-        k_bs_build_jobs<<<(unsigned)((m2 + 255) / 256), 256, 0, s>>>(L, *Ln, S, m2, k, jobs, ws, wss, npts);
+        k_bs_build_jobs<<<(unsigned)((m2 + 255) / 256), 256, 0, s>>>(L, *Ln, S, m2, k, jobs, ws, wss, npts,
+                                                                    use_spec ? pair_ws : nullptr, pair_wss);
         if (wss) {
             const uint64_t scratch_words = carry_scratch_bytes_n(npts) / 8;
             k_bs_zero_ws<<<(unsigned)m2, 256, 0, s>>>(jobs, m2, scratch_words);
@@ -498,11 +638,17 @@ static cudaError_t merge_level(Context* c, const LevelView& L, const uint64_t mx
         if ((e = cudaGetLastError()) != cudaSuccess) break;
         for (uint64_t off = 0; off < m2 && e == cudaSuccess; off += 65535) {
             const unsigned nj = (unsigned)std::min<uint64_t>(65535, m2 - off);
-            e = launch_bucket(p, jobs + off, nj, c->tw, c->d_err, s);
+            e = launch_bucket(p, jobs + off, nj, c->tw, c->d_err, s, use_spec);
+        }
+        if (!second) {
+            pair_ws = ws;  // job i's bufA starts its workspace slot
+            pair_wss = wss;
         }
     }
     *products += 4 * m2;
-    if (e == cudaSuccess && m2) {
+    if (e == cudaSuccess && m2 && m2 <= BS_GRID_MAX_MERGES && capT >= BS_GRID_MIN_LIMBS) {
+        e = signed_add_grid(c, S, L.sign, *Ln, m2, capT, s);
+    } else if (e == cudaSuccess && m2) {
         const uint64_t maxn = capT;
         unsigned threads = 32;
         while (threads < 1024 && (uint64_t)threads * ADD_LPT < maxn) threads <<= 1;

@@ -103,8 +103,28 @@ struct Tracer {
 //   ws: workspace of workspace_bytes_for(logn) bytes; err: device error word.
 // All passes, the carry and the bookkeeping of one size bucket of a batch:
 // `njobs` products of plan p whose pointers are in the device table `jobs`.
+// a_ready: every job's bufA already holds the finished forward spectrum of
+// its operand a under plan p (a spectrum several products share: the kernels
+// only read bufA), so a's forward passes are skipped. Plans of one CTA
+// (npass == 0) transform both operands themselves and ignore it.
 cudaError_t launch_bucket(const Plan& p, const ProdJob* jobs, unsigned njobs, const RootTables& tw, u32* err,
-                          cudaStream_t s);
+                          cudaStream_t s, bool a_ready = false);
+// Only the forward transform of operand a of each job, into its bufA
+// (npass >= 1): the spectrum that later launch_bucket(..., a_ready) calls read.
+cudaError_t launch_bucket_spectrum(const Plan& p, const ProdJob* jobs, unsigned njobs, const RootTables& tw,
+                                   cudaStream_t s);
+
+// Grid-wide passes over u32 limbs (b2m_bigops.cu), ordered on s:
+// out = a +- b mod 2^(32 n) (limbs of a at or past la read as 0, likewise b;
+// out may be a or b) with the carry or borrow out in *flag, using `scratch`
+// of addsub_scratch_bytes(n) bytes; *out = the largest k + 1 with a[k] != 0
+// (launch_top) or a[k] != b[k] (launch_top_diff) for k < n, into a word the
+// caller zeroed.
+uint64_t addsub_scratch_bytes(uint64_t n);
+cudaError_t launch_addsub(const u32* a, uint64_t la, const u32* b, uint64_t lb, uint64_t n, int sub, u32* out,
+                          void* scratch, u32* flag, cudaStream_t s);
+cudaError_t launch_top(const u32* a, uint64_t n, unsigned long long* out, cudaStream_t s);
+cudaError_t launch_top_diff(const u32* a, const u32* b, uint64_t n, unsigned long long* out, cudaStream_t s);
 
 // Zero `nwords` u64 of carry scratch and every job's out_len.
 cudaError_t launch_batch_prep(cudaStream_t s, const ProdJob* jobs, unsigned njobs, unsigned long long* scratch,

@@ -355,8 +355,35 @@ cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb,
     return e;
 }
 
+// Forward transform of operand `op` of every job (op 1 ends in the fused
+// pass: pointwise product with bufA and the first inverse pass).
+static cudaError_t bucket_forward(const Plan& p, const ProdJob* jobs, unsigned njobs, const RootTables& tw,
+                                  cudaStream_t s, int op, u64 ninv) {
+    const int logn = p.logn;
+    cudaError_t e = cudaSuccess;
+    int k0 = 0;
+    if (p.three) {
+        e = launch_r3_fwd(s, nullptr, 0, nullptr, logn, tw, jobs, njobs, op);
+    } else {
+        e = launch_fwd_first(p.logr[0], geo(p, 0), s, nullptr, 0, nullptr, tw, jobs, njobs, op);
+        k0 = 1;
+    }
+    for (int k = k0; e == cudaSuccess && k + 1 < p.npass; ++k)
+        e = launch_fwd_mid(p.logr[k], geo(p, k), s, nullptr, tw, jobs, njobs, op);
+    if (e != cudaSuccess) return e;
+    const int last = p.npass - 1;
+    return op == 0 ? launch_fwd_last(p.logr[last], geo(p, last), s, nullptr, tw, jobs, njobs)
+                   : launch_fused_last(p.logr[last], geo(p, last), s, nullptr, nullptr, ninv, tw, jobs, njobs);
+}
+
+cudaError_t launch_bucket_spectrum(const Plan& p, const ProdJob* jobs, unsigned njobs, const RootTables& tw,
+                                   cudaStream_t s) {
+    if (p.npass == 0) return cudaErrorInvalidValue;
+    return bucket_forward(p, jobs, njobs, tw, s, 0, 0);
+}
+
 cudaError_t launch_bucket(const Plan& p, const ProdJob* jobs, unsigned njobs, const RootTables& tw, u32* err,
-                          cudaStream_t s) {
+                          cudaStream_t s, bool a_ready) {
     const int logn = p.logn;
     const u64 ninv = gl_inv(plan_points(p));
     if (p.npass == 0) {
@@ -369,21 +396,8 @@ cudaError_t launch_bucket(const Plan& p, const ProdJob* jobs, unsigned njobs, co
         return launch_mul_small(logn, g, s, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, ninv, tw, jobs, njobs);
     }
     cudaError_t e = cudaSuccess;
-    for (int op = 0; op < 2 && e == cudaSuccess; ++op) {
-        int k0 = 0;
-        if (p.three) {
-            e = launch_r3_fwd(s, nullptr, 0, nullptr, logn, tw, jobs, njobs, op);
-        } else {
-            e = launch_fwd_first(p.logr[0], geo(p, 0), s, nullptr, 0, nullptr, tw, jobs, njobs, op);
-            k0 = 1;
-        }
-        for (int k = k0; e == cudaSuccess && k + 1 < p.npass; ++k)
-            e = launch_fwd_mid(p.logr[k], geo(p, k), s, nullptr, tw, jobs, njobs, op);
-        if (e != cudaSuccess) break;
-        const int last = p.npass - 1;
-        e = op == 0 ? launch_fwd_last(p.logr[last], geo(p, last), s, nullptr, tw, jobs, njobs)
-                    : launch_fused_last(p.logr[last], geo(p, last), s, nullptr, nullptr, ninv, tw, jobs, njobs);
-    }
+    for (int op = a_ready ? 1 : 0; op < 2 && e == cudaSuccess; ++op)
+        e = bucket_forward(p, jobs, njobs, tw, s, op, ninv);
     for (int k = p.npass - 2; e == cudaSuccess && k >= 0; --k)
         e = launch_inv_mid(p.logr[k], geo(p, k), s, nullptr, tw, jobs, njobs);
     if (e == cudaSuccess && p.three) e = launch_r3_inv(s, nullptr, logn, tw, jobs, njobs);
