@@ -26,6 +26,7 @@
 #include "b2m_internal.h"
 #include "carry.cuh"
 #include "ntt_engine.cuh"
+#include "school.cuh"
 
 namespace b2m {
 
@@ -250,10 +251,17 @@ k_fused_last(u64* __restrict__ bbuf, const u64* __restrict__ aspec, u64 ninv, Ro
 // ---------------------------------------------------------------------------
 // Whole product in one CTA for N = 2^LOGN <= 2^13: both transforms live in
 // shared memory, the carry is a block scan. max(1, N/16) threads; thread t
-// owns coefficients [t*G, (t+1)*G), G = min(16, N).
+// owns coefficients [t*G, (t+1)*G), G = min(16, N). A product whose
+// schoolbook cost is lower (school_cheaper) is computed that way instead, by
+// the same threads in the same shared memory.
 // ---------------------------------------------------------------------------
+constexpr int small_threads(int logn) { return logn >= 4 ? 1 << (logn - 4) : 1; }
+constexpr int small_min_blocks(int logn) {
+    return PASS_THREADS_MAX / small_threads(logn) < 32 ? PASS_THREADS_MAX / small_threads(logn) : 32;
+}
+
 template <int LOGN>
-__global__ void __launch_bounds__(512) k_mul_small(const u32* __restrict__ a, u64 na, const u32* __restrict__ b,
+__global__ void __launch_bounds__(small_threads(LOGN), small_min_blocks(LOGN)) k_mul_small(const u32* __restrict__ a, u64 na, const u32* __restrict__ b,
                                                    u64 nb, u32* __restrict__ out, u64 nout,
                                                    unsigned long long* out_len, u64 ninv, RootTables tw,
                                                    const ProdJob* __restrict__ jobs) {
@@ -274,6 +282,10 @@ __global__ void __launch_bounds__(512) k_mul_small(const u32* __restrict__ a, u6
     u64* smB = sm + RP;
     CState* s_st = reinterpret_cast<CState*>(sm + 2 * RP);
     __shared__ unsigned long long s_top;
+    if (school_cheaper(na, nb, LOGN)) {
+        school_cta(a, na, b, nb, out, out_len, reinterpret_cast<unsigned char*>(sm), s_st, &s_top);
+        return;
+    }
     const u64 nda = 2 * na, ndb = 2 * nb;
     for (int i = threadIdx.x; i < N; i += blockDim.x) {
         smA[TL::saddr(i, 0)] = digit_of(a, nda, i);
@@ -297,19 +309,28 @@ __global__ void __launch_bounds__(512) k_mul_small(const u32* __restrict__ a, u6
     for (int i = 0; i < G; ++i) v[i] = smB[TL::saddr((int)threadIdx.x * G + i, 0)];
     u32 lm[G / 2];
     const CState st = group_carry<G>(v, lm);
-    s_st[threadIdx.x] = st;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        // Serial exclusive scan (T <= 512): s_st[t].h becomes the carry into t.
-        u64 c = 0;
-        for (int t = 0; t < T; ++t) {
-            const CState f = s_st[t];
-            s_st[t].h = c;
-            c = cs_eval(f, c);
+    u64 cin;
+    if (T >= 32) {
+        bool has;
+        CState agg;
+        const CState ex = block_scan_carry(st, &has, &agg, s_st);
+        cin = has ? cs_eval(ex, 0) : 0;
+    } else {
+        s_st[threadIdx.x] = st;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            // Serial exclusive scan: s_st[t].h becomes the carry into t.
+            u64 c = 0;
+            for (int t = 0; t < T; ++t) {
+                const CState f = s_st[t];
+                s_st[t].h = c;
+                c = cs_eval(f, c);
+            }
         }
+        __syncthreads();
+        cin = s_st[threadIdx.x].h;
     }
-    __syncthreads();
-    group_add_carry<G / 2>(lm, s_st[threadIdx.x].h);
+    group_add_carry<G / 2>(lm, cin);
     const u64 lbase = (u64)threadIdx.x * (G / 2);
     unsigned long long top = 0;
 #pragma unroll
