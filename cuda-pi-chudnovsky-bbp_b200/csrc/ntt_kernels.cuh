@@ -216,6 +216,7 @@ k_fwd_last(u64* __restrict__ buf, RootTables tw, const ProdJob* __restrict__ job
 
 // Last forward pass of operand B, pointwise product with A's spectrum (same
 // positions) and N^-1, then the first inverse pass -- one tile, one kernel.
+// aspec null (no job table): a square, B's spectrum times itself.
 template <int LOGR, int LOGC>
 __global__ void B2M_PASS_BOUNDS((Tile<LOGR, LOGC, MAP_ROW>::T))
 k_fused_last(u64* __restrict__ bbuf, const u64* __restrict__ aspec, u64 ninv, RootTables tw,
@@ -227,8 +228,9 @@ k_fused_last(u64* __restrict__ bbuf, const u64* __restrict__ aspec, u64 ninv, Ro
         bbuf = jobs[blockIdx.y].bufB;
         aspec = jobs[blockIdx.y].bufA;
     }
+    const bool square = aspec == nullptr;
     bbuf += blockIdx.z * zstride;
-    aspec += blockIdx.z * zstride;
+    if (!square) aspec += blockIdx.z * zstride;
     const G gp;
     const u64 off = ((u64)blockIdx.x << (LOGR + LOGC)) + threadIdx.x;
     u64* base = bbuf + off;
@@ -237,10 +239,18 @@ k_fused_last(u64* __restrict__ bbuf, const u64* __restrict__ aspec, u64 ninv, Ro
     for (int k = 0; k < G::PER; ++k) sm[gp.sa0 + G::soff(k)] = base[k * TL::T];
     __syncthreads();
     tile_fwd<TL>(sm, tw.dtw);
+    if (square) {
 #pragma unroll
-    for (int k = 0; k < G::PER; ++k) {
-        u64& v = sm[gp.sa0 + G::soff(k)];
-        v = gl_mul(gl_mul(v, __ldg(abase + k * TL::T)), ninv);
+        for (int k = 0; k < G::PER; ++k) {
+            u64& v = sm[gp.sa0 + G::soff(k)];
+            v = gl_mul(gl_mul(v, v), ninv);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < G::PER; ++k) {
+            u64& v = sm[gp.sa0 + G::soff(k)];
+            v = gl_mul(gl_mul(v, __ldg(abase + k * TL::T)), ninv);
+        }
     }
     __syncthreads();
     tile_inv<TL>(sm, tw.dtw);

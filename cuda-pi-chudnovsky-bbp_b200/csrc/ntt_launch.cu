@@ -338,9 +338,15 @@ cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb,
     unsigned long long* ol = out_len ? reinterpret_cast<unsigned long long*>(out_len) : len_tmp;
     if (out_len && (e = cudaMemsetAsync(out_len, 0, sizeof(uint64_t), s)) != cudaSuccess) return e;
 
-    if ((e = launch_forward(a, na, bufA, p, tw, false, nullptr, 0, s, tr)) != cudaSuccess) return e;
-    if (b_ready && (e = cudaStreamWaitEvent(s, b_ready, 0)) != cudaSuccess) return e;
-    if ((e = launch_forward(b, nb, bufB, p, tw, true, bufA, ninv, s, tr)) != cudaSuccess) return e;
+    if (a == b && na == nb) {
+        // a square: one forward transform, its spectrum squared in the fused pass
+        if (b_ready && (e = cudaStreamWaitEvent(s, b_ready, 0)) != cudaSuccess) return e;
+        if ((e = launch_forward(b, nb, bufB, p, tw, true, nullptr, ninv, s, tr)) != cudaSuccess) return e;
+    } else {
+        if ((e = launch_forward(a, na, bufA, p, tw, false, nullptr, 0, s, tr)) != cudaSuccess) return e;
+        if (b_ready && (e = cudaStreamWaitEvent(s, b_ready, 0)) != cudaSuccess) return e;
+        if ((e = launch_forward(b, nb, bufB, p, tw, true, bufA, ninv, s, tr)) != cudaSuccess) return e;
+    }
     for (int k = p.npass - 2; k >= 0; --k) {
         if (tr) tr->mark(s, B2M_K_INV_MID, p.logr[k]);
         if ((e = launch_inv_mid(p.logr[k], geo(p, k), s, bufB, tw)) != cudaSuccess) return e;

@@ -15,7 +15,10 @@ namespace b2m {
 
 // Products whose schoolbook cost is below this many limb multiply-adds per
 // transform point and level of the NTT they would otherwise use.
-constexpr unsigned long long SCHOOL_MACS_PER_POINT_LEVEL = 16;
+#ifndef B2M_SCHOOL_MACS_PER_POINT_LEVEL
+#define B2M_SCHOOL_MACS_PER_POINT_LEVEL 16
+#endif
+constexpr unsigned long long SCHOOL_MACS_PER_POINT_LEVEL = B2M_SCHOOL_MACS_PER_POINT_LEVEL;
 
 __device__ __forceinline__ bool school_cheaper(u64 na, u64 nb, int logn) {
     return na * nb <= ((1ull << logn) * (unsigned long long)logn) * SCHOOL_MACS_PER_POINT_LEVEL;

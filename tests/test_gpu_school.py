@@ -1,4 +1,4 @@
-"""The schoolbook path of the one-CTA product kernel.
+"""The schoolbook path of the one-CTA product kernel, and squares.
 
 Products of at most 2^13 transform points whose na * nb is below about
 16 N log2 N limb multiply-adds are computed by schoolbook columns (96-bit
@@ -59,3 +59,28 @@ def test_school_in_one_batch(b2m_gpu):
         want = oracle.mul_port(a, b)
         n = int(lens[i].item())
         assert n == want.size and np.array_equal(o.cpu().numpy().view(np.uint32)[:n], want), sizes[i]
+
+
+@pytest.mark.parametrize("n", [3000, 8192, 20000, 40000, 100000, 300000, 1 << 20, 1 << 23])
+@pytest.mark.parametrize("kind", [0, 1])
+def test_square_through_one_pointer(b2m_gpu, n, kind):
+    """a * a with both operands at one device pointer takes the squaring path
+    (one forward transform, its spectrum squared in the fused pass) on two-
+    and three-pass and 3 * 2^k plans."""
+    import torch
+
+    a = gen_operand(n + 11, n, kind)
+    d = torch.from_numpy(a.view(np.int32)).cuda()
+    out = torch.zeros(2 * n, dtype=torch.int32, device="cuda")
+    olen = torch.zeros(1, dtype=torch.int64, device="cuda")
+    b2m_gpu.mul_device(d.data_ptr(), n, d.data_ptr(), n, out.data_ptr(), 2 * n, olen.data_ptr(), 0)
+    b2m_gpu.stream_check(0)
+    got = out.cpu().numpy().view(np.uint32)[: int(olen.item())]
+    if n <= 100000:
+        assert np.array_equal(got, oracle.mul_port(a, a))
+    else:
+        ia = int.from_bytes(a.tobytes(), "little")
+        ip = int.from_bytes(got.tobytes(), "little")
+        for q in [(1 << 61) - 1, (1 << 32) + 1, (1 << 32) - 1]:
+            assert ip % q == (ia % q) * (ia % q) % q
+        assert np.array_equal(got[:32], oracle.mul_port(a[:32], a[:32])[:32])
