@@ -1,7 +1,7 @@
 """The schoolbook path of the one-CTA product kernel, and squares.
 
-Products of at most 2^13 transform points whose na * nb is below about
-16 N log2 N limb multiply-adds are computed by schoolbook columns (96-bit
+Products of at most 2^13 transform points whose na * nb is at most 128 N
+limb multiply-adds are computed by schoolbook columns (96-bit
 column sums, a block scan of carry functions) instead of the one-CTA NTT.
 These cases sit on both sides of that choice at every one-CTA length, with
 the operands that stress it most: all-0xFFFFFFFF limbs (the largest column
