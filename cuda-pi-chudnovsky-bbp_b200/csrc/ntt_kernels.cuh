@@ -36,6 +36,17 @@ constexpr int PASS_THREADS_MAX = 1024;
 // (64 registers a thread), whatever the tile's thread count.
 #define B2M_PASS_BOUNDS(T) __launch_bounds__((T), (PASS_THREADS_MAX / (T)))
 
+// Asynchronous 8-byte copy global -> shared (no register staging, so a
+// thread keeps all of its tile loads in flight), and the wait for all of the
+// thread's copies.
+__device__ __forceinline__ void cp_async8(u64* smem_dst, const u64* gsrc) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 __device__ __forceinline__ u64 digit_of(const u32* __restrict__ limbs, u64 ndig, u64 n) {
     if (n >= ndig) return 0;
     const u32 w = __ldg(limbs + (n >> 1));
@@ -144,7 +155,8 @@ k_fwd_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const u64* _
     buf += blockIdx.z * zstride;  // sub-transform of a radix-3 plan
     const G gp(logS, logM);
 #pragma unroll
-    for (int k = 0; k < G::PER; ++k) sm[gp.sa0 + G::soff(k)] = buf[gp.gi0 + k * gp.gstep];
+    for (int k = 0; k < G::PER; ++k) cp_async8(sm + gp.sa0 + G::soff(k), buf + gp.gi0 + k * gp.gstep);
+    cp_async_wait_all();
     __syncthreads();
     tile_fwd<TL>(sm, tw.dtw);
     if (ttab) {
@@ -175,17 +187,27 @@ k_inv_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const u64* _
     if (jobs) buf = jobs[blockIdx.y].bufB;
     buf += blockIdx.z * zstride;
     const G gp(logS, logM);
-    if (ttab) {
+    // the tile arrives by asynchronous copies while the twiddles load; each
+    // thread then multiplies the elements it copied
 #pragma unroll
-        for (int k = 0; k < G::PER; ++k)
-            sm[gp.sa0 + G::soff(k)] = gl_mul(buf[gp.gi0 + k * gp.gstep], __ldg(ttab + gp.ti0 + k * gp.gstep));
-    } else {
+    for (int k = 0; k < G::PER; ++k) cp_async8(sm + gp.sa0 + G::soff(k), buf + gp.gi0 + k * gp.gstep);
+    if (ttab) {
+        u64 t[G::PER];
+#pragma unroll
+        for (int k = 0; k < G::PER; ++k) t[k] = __ldg(ttab + gp.ti0 + k * gp.gstep);
+        cp_async_wait_all();
 #pragma unroll
         for (int k = 0; k < G::PER; ++k) {
-            u64 x = buf[gp.gi0 + k * gp.gstep];
+            u64& v = sm[gp.sa0 + G::soff(k)];
+            v = gl_mul(v, t[k]);
+        }
+    } else {
+        cp_async_wait_all();
+#pragma unroll
+        for (int k = 0; k < G::PER; ++k) {
             const u32 e = gp.e0 + G::fk(k) * gp.ec;
-            if (e) x = gl_mul(x, uroot(0u - e, tw.u1, tw.u2));
-            sm[gp.sa0 + G::soff(k)] = x;
+            u64& v = sm[gp.sa0 + G::soff(k)];
+            if (e) v = gl_mul(v, uroot(0u - e, tw.u1, tw.u2));
         }
     }
     __syncthreads();
@@ -207,7 +229,8 @@ k_fwd_last(u64* __restrict__ buf, RootTables tw, const ProdJob* __restrict__ job
     const G gp;
     u64* base = buf + ((u64)blockIdx.x << (LOGR + LOGC)) + threadIdx.x;
 #pragma unroll
-    for (int k = 0; k < G::PER; ++k) sm[gp.sa0 + G::soff(k)] = base[k * TL::T];
+    for (int k = 0; k < G::PER; ++k) cp_async8(sm + gp.sa0 + G::soff(k), base + k * TL::T);
+    cp_async_wait_all();
     __syncthreads();
     tile_fwd<TL>(sm, tw.dtw);
 #pragma unroll
@@ -236,7 +259,8 @@ k_fused_last(u64* __restrict__ bbuf, const u64* __restrict__ aspec, u64 ninv, Ro
     u64* base = bbuf + off;
     const u64* abase = aspec + off;
 #pragma unroll
-    for (int k = 0; k < G::PER; ++k) sm[gp.sa0 + G::soff(k)] = base[k * TL::T];
+    for (int k = 0; k < G::PER; ++k) cp_async8(sm + gp.sa0 + G::soff(k), base + k * TL::T);
+    cp_async_wait_all();
     __syncthreads();
     tile_fwd<TL>(sm, tw.dtw);
     if (square) {
