@@ -30,9 +30,10 @@ namespace b2m {
 // Default plans for 2^14..2^27 points: the autotuner's fastest candidate on
 // a B200 for a square product of each length (uniform random limbs, median
 // of three). Small lengths favour 2^12-element tiles (more CTAs for little
-// work); 2^20..2^24 two passes with a 2^12..2^13 contiguous last pass;
-// 2^25 and up three passes of 2^12-element tiles, whose extra HBM sweep
-// costs less than the latency one 2^14-element CTA per SM leaves exposed.
+// work); 2^19..2^21 two passes with a 2^11..2^12 contiguous last pass; 2^22
+// and up (and 2^23 within 0.4%) three passes of 2^12-element tiles, whose
+// extra HBM sweep costs less than the latency that one 2^14-element CTA per
+// SM leaves exposed.
 namespace {
 struct DefaultPlan {
     int npass, r0, r1, r2, tile;
@@ -42,17 +43,17 @@ constexpr DefaultPlan kDefaultPlans[DEFAULT_MAX_LOGN - DEFAULT_MIN_LOGN + 1] = {
     {2, 8, 6, 0, 12},    // 2^14
     {2, 7, 8, 0, 12},    // 2^15
     {2, 8, 8, 0, 12},    // 2^16
-    {2, 9, 8, 0, 12},    // 2^17
-    {2, 6, 12, 0, 12},   // 2^18
+    {2, 8, 9, 0, 12},    // 2^17
+    {2, 7, 11, 0, 12},   // 2^18
     {2, 7, 12, 0, 12},   // 2^19
     {2, 8, 12, 0, 13},   // 2^20
     {2, 9, 12, 0, 13},   // 2^21
-    {2, 10, 12, 0, 12},  // 2^22
+    {3, 6, 8, 8, 12},    // 2^22
     {2, 10, 13, 0, 13},  // 2^23
-    {2, 11, 13, 0, 13},  // 2^24
+    {3, 8, 8, 8, 12},    // 2^24
     {3, 9, 8, 8, 12},    // 2^25
     {3, 9, 9, 8, 12},    // 2^26
-    {3, 9, 7, 11, 12},   // 2^27
+    {3, 8, 8, 11, 12},   // 2^27
 };
 }  // namespace
 
