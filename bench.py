@@ -238,7 +238,7 @@ def run_ours(args) -> None:
     sp = stream.cuda_stream
     # Plan choice (pass split, tile size) timed once before any measurement;
     # every later product of this transform length uses the fastest.
-    tune = [] if args.no_autotune else b200mul.autotune(na, nb, sp)
+    tune = b200mul.autotune(na, nb, sp) if args.autotune and not args.no_autotune else []
     plan = b200mul.plan_describe(na, nb)
     n = plan["points"]
 
@@ -768,7 +768,10 @@ def main():
     ap.add_argument("--trace-steps", type=int, default=10)
     ap.add_argument("--cpu-sample-log", type=int, default=22)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-autotune", action="store_true", help="single: keep the default plan")
+    ap.add_argument("--autotune", action="store_true",
+                    help="single: time every candidate plan first and keep the fastest (the default plan of each "
+                         "length is already the measured fastest; candidates within noise of it may win)")
+    ap.add_argument("--no-autotune", action="store_true", help="single: keep the default plan (the default)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
