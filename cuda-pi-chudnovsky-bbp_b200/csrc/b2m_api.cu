@@ -535,18 +535,29 @@ b2m_status b2m_mul_host(const uint32_t* a, uint64_t na, const uint32_t* b, uint6
     cudaStream_t s = c->hstream;
     cudaError_t e;
     if ((e = twtable_ensure(c, p, s)) != cudaSuccess) return cuda_status(e, "twiddle table");
-    // Operand B crosses the bus after A, on a second stream, while A's forward
-    // transform runs: the product waits for B only before B's transform.
-    if ((e = cudaMemcpyAsync(da, a, 4 * na, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-        (e = cudaEventRecord(c->hev_a, s)) != cudaSuccess ||
-        (e = cudaStreamWaitEvent(c->hcopy, c->hev_a, 0)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(db, b, 4 * nb, cudaMemcpyHostToDevice, c->hcopy)) != cudaSuccess ||
-        (e = cudaEventRecord(c->hev_b, c->hcopy)) != cudaSuccess)
-        return cuda_status(e, "cudaMemcpyAsync(H2D)");
-    if ((e = launch_product(da, na, db, nb, dout, dlen, ws, p, c->tw, c->d_err, s, nullptr, c->hev_b)) !=
-        cudaSuccess) {
-        cudaStreamSynchronize(c->hcopy);
-        return cuda_status(e, "kernel launch");
+    if (a == b && na == nb) {
+        // a square (the reference's x * x passes one vector twice): one copy,
+        // one forward transform (launch_product's squaring path)
+        if ((e = cudaMemcpyAsync(da, a, 4 * na, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+            return cuda_status(e, "cudaMemcpyAsync(H2D)");
+        if ((e = launch_product(da, na, da, na, dout, dlen, ws, p, c->tw, c->d_err, s, nullptr, nullptr)) !=
+            cudaSuccess)
+            return cuda_status(e, "kernel launch");
+    } else {
+        // Operand B crosses the bus after A, on a second stream, while A's
+        // forward transform runs: the product waits for B only before B's
+        // transform.
+        if ((e = cudaMemcpyAsync(da, a, 4 * na, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+            (e = cudaEventRecord(c->hev_a, s)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(c->hcopy, c->hev_a, 0)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(db, b, 4 * nb, cudaMemcpyHostToDevice, c->hcopy)) != cudaSuccess ||
+            (e = cudaEventRecord(c->hev_b, c->hcopy)) != cudaSuccess)
+            return cuda_status(e, "cudaMemcpyAsync(H2D)");
+        if ((e = launch_product(da, na, db, nb, dout, dlen, ws, p, c->tw, c->d_err, s, nullptr, c->hev_b)) !=
+            cudaSuccess) {
+            cudaStreamSynchronize(c->hcopy);
+            return cuda_status(e, "kernel launch");
+        }
     }
     uint64_t hlen = 0;
     if ((e = cudaMemcpyAsync(out, dout, 4 * (na + nb), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||

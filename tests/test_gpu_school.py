@@ -84,3 +84,18 @@ def test_square_through_one_pointer(b2m_gpu, n, kind):
         for q in [(1 << 61) - 1, (1 << 32) + 1, (1 << 32) - 1]:
             assert ip % q == (ia % q) * (ia % q) % q
         assert np.array_equal(got[:32], oracle.mul_port(a[:32], a[:32])[:32])
+
+
+@pytest.mark.parametrize("n", [1000, 5000, 40000, 300000])
+def test_square_through_the_host_call(b2m_gpu, n):
+    """The reference-facing host call given one array twice (the reference's
+    x * x) copies it once and squares it."""
+    a = gen_operand(n + 29, n, 1 if n == 5000 else 0)
+    p = b2m_gpu.mul_ntt_cuda(a, a)
+    if n <= 40000:
+        assert np.array_equal(p, oracle.mul_port(a, a))
+    else:
+        ia = int.from_bytes(a.tobytes(), "little")
+        ip = int.from_bytes(p.tobytes(), "little")
+        for q in [(1 << 61) - 1, (1 << 32) + 1, (1 << 32) - 1]:
+            assert ip % q == (ia % q) * (ia % q) % q
