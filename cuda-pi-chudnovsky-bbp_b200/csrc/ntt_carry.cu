@@ -29,7 +29,7 @@ __device__ __forceinline__ void st_release(u32* p, u32 v) {
 
 constexpr int LOOKBACK_SPIN_LIMIT = 1 << 22;
 
-__global__ void __launch_bounds__(CARRY_THREADS) k_carry(const u64* __restrict__ coef, u32* __restrict__ out,
+__global__ void __launch_bounds__(CARRY_THREADS, 8) k_carry(const u64* __restrict__ coef, u32* __restrict__ out,
                                                          u64 nout, LookbackSlot* slots, u32* ticket,
                                                          unsigned long long* out_len, u32* err,
                                                          const ProdJob* __restrict__ jobs) {
