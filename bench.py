@@ -123,7 +123,7 @@ class ClockSampler:
 # ---------------------------------------------------------------------------- CPU
 def _ref_or_port():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle  # the checker: only the CPU-baseline leg of this script uses it
+    import oracle  # the checker: only the CPU-baseline leg and the reference arm use it
 
     if oracle.ref_available():
         return oracle, "reference", lambda a, b: oracle.mul_ref(a, b, "ntt-cpu")
@@ -136,72 +136,71 @@ def nlogn_scale(n_from: int, n_to: int) -> float:
     return (nt * math.log2(nt)) / (nf * math.log2(nf))
 
 
-def cpu_products(sample_limbs: int, threads: int, fn) -> float:
-    """Run `threads` concurrent sample products (ctypes releases the GIL);
-    returns the wall time in seconds."""
-    import numpy as np
-    from b200mul import gen_operand
-
-    ops = [(gen_operand(SEED_A + i, sample_limbs), gen_operand(SEED_B + i, sample_limbs)) for i in range(threads)]
-    res = [None] * threads
-
-    def work(i):
-        res[i] = fn(*ops[i])
-
-    ts = [threading.Thread(target=work, args=(i,)) for i in range(threads)]
+def cpu_product_s(oracle_mod, fn, na: int, nb: int, seed_a: int = SEED_A, seed_b: int = SEED_B) -> float:
+    """Wall time of one CPU product of the seeded operands (the same splitmix64
+    operands the GPU arm multiplies, made by the oracle's C generator so that
+    the product library is never loaded here)."""
+    a = oracle_mod.gen_operand(seed_a, na)
+    b = oracle_mod.gen_operand(seed_b, nb)
     t0 = time.perf_counter()
-    for t in ts:
-        t.start()
-    for t in ts:
-        t.join()
+    p = fn(a, b)
     dt = time.perf_counter() - t0
-    assert all(r is not None and r.size == 2 * sample_limbs for r in res) and np is not None
+    if p.size not in (na + nb, na + nb - 1):
+        raise RuntimeError("CPU product has the wrong length")
     return dt
 
 
-def cpu_baseline(sample_log: int = 22) -> dict:
+def cpu_baseline(sample_log: int = 24) -> dict:
     """The reference's CPU NTT (single-threaded, as the reference is) on one
-    sample product, scaled to the 2^24-limb metric by N log2 N."""
-    _, kind, fn = _ref_or_port()
+    product; at the default sample_log = 24 that is the headline 2^24 x 2^24
+    product itself (about a minute), measured, not scaled."""
+    oracle_mod, kind, fn = _ref_or_port()
     n = 1 << sample_log
-    dt = cpu_products(n, 1, fn)
+    dt = cpu_product_s(oracle_mod, fn, n, n)
     scale = nlogn_scale(n, NA)
-    return {"value": round(dt * 1e3 * scale, 1), "unit": "ms", "cores": 1, "kind": kind,
-            "sample": f"one {n}x{n}-limb product (mul_ntt_cpu, 1 thread) in {dt:.2f} s, scaled to "
-                      f"2^24 limbs by N log2 N (x{scale:.2f})"}
+    sample = (f"one {n}x{n}-limb product (mul_ntt_cpu, src/ntt_cpu.cpp:111-129, 1 thread) in {dt:.2f} s"
+              + ("" if n == NA else f", scaled to 2^24 limbs by N log2 N (x{scale:.2f})"))
+    return {"value": round(dt * 1e3 * scale, 1), "unit": "ms", "cores": 1, "kind": kind, "sample": sample,
+            "measured_full_size": n == NA}
 
 
 def run_reference(args) -> None:
+    """The reference's own CPU implementation of the path (mul_ntt_cpu,
+    src/ntt_cpu.cpp:111-129, compiled from the reference's sources into
+    oracle/_ref) on this host. The reference multiplies on one thread and has
+    no parallel path, so one product uses one core. `value` is one measured
+    2^24 x 2^24 product, the headline workload itself. The K timed steps are
+    bounded samples of the same routine (2^20 x 2^20 limbs each, about 3 s),
+    so that the whole run stays within a few minutes; their N log2 N scaling
+    to 2^24 limbs is reported beside the measured value, not as it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    _, kind, fn = _ref_or_port()
-    threads = os.cpu_count() or 1
-    # Size each step so that warmup + steps stay near two minutes.
-    budget = 120.0 / max(1, args.steps + args.warmup)
-    t_cal = cpu_products(1 << 16, 1, fn)
-    lg = 16
-    while lg < 24 and t_cal * nlogn_scale(1 << 16, 1 << (lg + 1)) * 1.15 <= budget:
-        lg += 1
-    n = 1 << lg
-    for _ in range(args.warmup):
-        cpu_products(n, threads, fn)
-    times = [cpu_products(n, threads, fn) for _ in range(args.steps)]
+    oracle_mod, kind, fn = _ref_or_port()
+    full_s = cpu_product_s(oracle_mod, fn, NA, NB)
+    sl = 1 << 20
+    for i in range(args.warmup):
+        cpu_product_s(oracle_mod, fn, 1 << 16, 1 << 16, SEED_A + i, SEED_B + i)
+    times = [cpu_product_s(oracle_mod, fn, sl, sl, SEED_A + i, SEED_B + i) for i in range(args.steps)]
     step = statistics.mean(times)
-    scale = nlogn_scale(n, NA)
-    value = step / threads * 1e3 * scale
+    value = full_s * 1e3
     out = {
-        "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": "ms", "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": "ms", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step * 1e3, 2),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (GF(p), p=2^64-2^32+1)",
-        "data": "synthetic: seeded uniform random u32 limbs",
+        "data": "synthetic: seeded uniform random u32 limbs (splitmix64, the GPU arm's operands)",
         "config": {"workload": "2^24 x 2^24-limb product, uniform random limbs", "na": NA, "nb": NB,
-                   "sample_limbs": n, "threads": threads},
-        "cpu_baseline": {"value": round(value, 2), "unit": "ms", "cores": threads, "kind": kind,
-                         "sample": f"each step: {threads} concurrent {n}x{n}-limb products of the reference's "
-                                   f"mul_ntt_cpu (src/ntt_cpu.cpp:111-129), one per host thread; ms per product "
-                                   f"= step wall / {threads}, scaled to 2^24 limbs by N log2 N (x{scale:.2f})"},
-        "e2e": {"value": round(value, 2), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                   "threads": 1, "host_threads_available": os.cpu_count()},
+        "full_size_product_ms": round(value, 1),
+        "steps_sample": {"limbs": sl, "mean_ms": round(step * 1e3, 1),
+                         "scaled_to_2^24_ms": round(step * 1e3 * nlogn_scale(sl, NA), 1),
+                         "note": "each timed step is one 2^20 x 2^20-limb product of the same routine; "
+                                 "the headline value above is the measured full-size product"},
+        "cpu_baseline": {"value": round(value, 1), "unit": "ms", "cores": 1, "kind": kind,
+                         "sample": f"one 2^24 x 2^24-limb product of the reference's mul_ntt_cpu "
+                                   f"(src/ntt_cpu.cpp:111-129), measured in {full_s:.1f} s on one thread "
+                                   f"(the reference has no multi-threaded product)"},
+        "e2e": {"value": round(value, 1), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
 
@@ -766,7 +765,8 @@ def main():
     ap.add_argument("--nb", type=int, default=NB)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--trace-steps", type=int, default=10)
-    ap.add_argument("--cpu-sample-log", type=int, default=22)
+    ap.add_argument("--cpu-sample-log", type=int, default=24,
+                    help="log2 limbs of the CPU-baseline product (24: the headline product itself)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--autotune", action="store_true",
                     help="single: time every candidate plan first and keep the fastest (the default plan of each "

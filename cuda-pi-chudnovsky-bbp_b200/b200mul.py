@@ -219,6 +219,21 @@ def selftest_wait_timeout(stream: int = 0) -> int:
     return int(lib.b2m_selftest_wait_timeout(stream or None))
 
 
+_sig("b2m_field_eval_host", ctypes.c_int, [ctypes.c_int, _u64p, _u64p, _u64p, ctypes.c_uint64])
+FIELD_OPS = {"add": 0, "sub": 1, "mul": 2, "shl": 3, "pow": 4, "inv": 5, "dft8": 6, "idft8": 7}
+
+
+def field_eval(op: str, a, b=None) -> np.ndarray:
+    """The device field arithmetic of the kernels, element-wise
+    (b2m_field_eval_host): op in FIELD_OPS, a and b u64 arrays."""
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.uint64))
+    b = np.zeros_like(a) if b is None else np.ascontiguousarray(np.asarray(b, dtype=np.uint64))
+    out = np.zeros_like(a)
+    check(lib.b2m_field_eval_host(FIELD_OPS[op], a.ctypes.data_as(_u64p), b.ctypes.data_as(_u64p),
+                                  out.ctypes.data_as(_u64p), a.size), "b2m_field_eval_host")
+    return out
+
+
 _sig("b2m_set_plan", ctypes.c_int, [ctypes.POINTER(PlanDesc)])
 
 

@@ -131,6 +131,29 @@ b2m_status b2m_stream_check(b2m_stream stream);
  * usable. Nothing faults, traps or hangs. */
 b2m_status b2m_selftest_wait_timeout(b2m_stream stream);
 
+/* Element-wise evaluation of the device field arithmetic that the transforms
+ * are built from (the Goldilocks field of include/goldilocks.h:90-189, which
+ * the reference's self-test checks in tests/self_test.cu:46-62): out[i] =
+ * op(a[i], b[i]) computed on the device by exactly the device functions the
+ * kernels inline. Host buffers of n elements, synchronous. Operands are field
+ * elements in [0, p) (SHL: b[i] is the shift amount, taken mod 192; POW: b[i]
+ * is the exponent; INV ignores b). DFT8 / IDFT8 transform each group of 8
+ * consecutive elements of a (n a multiple of 8; b unused): the forward
+ * 8-point DFT with root 2^24, natural order in, bit-reversed order out, and
+ * its unscaled inverse (bit-reversed in, natural out, root 2^-24).
+ * Results are canonical, in [0, p). */
+typedef enum b2m_field_op {
+    B2M_FIELD_ADD = 0,
+    B2M_FIELD_SUB = 1,
+    B2M_FIELD_MUL = 2,
+    B2M_FIELD_SHL = 3,   /* a * 2^(b mod 192) */
+    B2M_FIELD_POW = 4,
+    B2M_FIELD_INV = 5,
+    B2M_FIELD_DFT8 = 6,
+    B2M_FIELD_IDFT8 = 7
+} b2m_field_op;
+b2m_status b2m_field_eval_host(int op, const uint64_t* a, const uint64_t* b, uint64_t* out, uint64_t n);
+
 /* ---- batched products ---------------------------------------------------------
  * No counterpart in the reference, whose tree (src/chudnovsky.cpp:64-102)
  * multiplies one pair at a time, each call paying its own allocation, copies

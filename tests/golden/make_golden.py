@@ -4,6 +4,9 @@ from the reference sources).
 
     python tests/golden/make_golden.py small      # field, self-test pairs, C1, sweep <= 2^20
     python tests/golden/make_golden.py large      # sweep 2^22 and 2^24 (minutes)
+    python tests/golden/make_golden.py odd        # sweep 2^17, 2^19, 2^21, 2^23 (minutes)
+    python tests/golden/make_golden.py xl         # sweep 2^25 .. 2^27 (about an hour of CPU,
+                                                  # three worker processes, ~13 GB each at 2^27)
     python tests/golden/make_golden.py chudnovsky # P/Q/T of the binary-splitting trees
     python tests/golden/make_golden.py pi         # digit strings of compute_pi_chudnovsky
 
@@ -29,7 +32,7 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 import oracle  # noqa: E402
 from golden_util import (gen_operand, selftest_pairs, sha_limbs, SWEEP_SMALL, SWEEP_LARGE,  # noqa: E402
-                         GL_P)
+                         SWEEP_ODD, SWEEP_XL, GL_P)
 
 
 def dump(name, obj):
@@ -81,6 +84,33 @@ def make_sweep(entries, name):
                           "1 thread of this container's host", "products": out})
 
 
+def _sweep_row(e):
+    a = gen_operand(e["seed_a"], e["na"], e["kind_a"])
+    b = gen_operand(e["seed_b"], e["nb"], e["kind_b"])
+    t = time.time()
+    p = oracle.mul_ref(a, b, "ntt-cpu")
+    dt = time.time() - t
+    r = dict(e)
+    r.update({"len": int(p.size), "sha256": sha_limbs(p), "ref_ntt_cpu_s": round(dt, 3)})
+    print(e["name"], p.size, f"{dt:.2f}s", flush=True)
+    return r
+
+
+def make_sweep_parallel(entries, name, workers):
+    """The same rows as make_sweep, one reference product per worker process
+    (each product is single-threaded), largest first."""
+    import multiprocessing as mp
+
+    order = sorted(range(len(entries)), key=lambda i: -(entries[i]["na"] + entries[i]["nb"]))
+    with mp.get_context("spawn").Pool(workers) as pool:
+        rows = pool.map(_sweep_row, [entries[i] for i in order], chunksize=1)
+    out = [None] * len(entries)
+    for i, r in zip(order, rows):
+        out[i] = r
+    dump(name, {"source": "reference mul_ntt_cpu (src/ntt_cpu.cpp:111-129) via oracle/_ref, "
+                          "1 thread of this container's host per product", "products": out})
+
+
 def make_chudnovsky(digit_list):
     ref = oracle.ref_lib()
     rows = []
@@ -103,7 +133,9 @@ def make_chudnovsky(digit_list):
 
 
 def make_pi(digit_list):
-    rows = []
+    path = os.path.join(HERE, "pi_digits.json")
+    old = json.load(open(path))["runs"] if os.path.exists(path) else []
+    rows = [r for r in old if r["digits"] not in digit_list]
     for d in digit_list:
         t = time.time()
         s = oracle.compute_pi_ref(d)
@@ -111,7 +143,7 @@ def make_pi(digit_list):
                      "head": s[:102], "ref_s": round(time.time() - t, 2)})
         print("pi", d, f"{time.time() - t:.1f}s", flush=True)
     dump("pi_digits.json", {"source": "reference compute_pi_chudnovsky (src/chudnovsky.cpp:107-164) via "
-                                      "oracle/_ref", "runs": rows})
+                                      "oracle/_ref", "runs": sorted(rows, key=lambda r: r["digits"])})
 
 
 if __name__ == "__main__":
@@ -122,6 +154,10 @@ if __name__ == "__main__":
         make_sweep(SWEEP_SMALL, "sweep_small.json")
     if "large" in what:
         make_sweep(SWEEP_LARGE, "sweep_large.json")
+    if "odd" in what:
+        make_sweep_parallel(SWEEP_ODD, "sweep_odd.json", 4)
+    if "xl" in what:
+        make_sweep_parallel(SWEEP_XL, "sweep_xl.json", 3)
     if "chudnovsky" in what:
         make_chudnovsky([1000, 100000, 1000000])
     if "chudnovsky10m" in what:
@@ -130,3 +166,5 @@ if __name__ == "__main__":
         make_pi([1000, 3500, 10000, 100000])
     if "pi1m" in what:
         make_pi([1000, 3500, 10000, 100000, 1000000])
+    if "pi3m" in what:
+        make_pi([3000000])

@@ -6,9 +6,10 @@
   na, nb = 1 + rnd32() % 1500 and limbs from rnd32(), normalised (:64-72).
 * ``gen_operand`` is the seeded operand generator (numpy copy; the product has
   one in b200mul.py and the oracle one in C -- the tests compare all three).
-* ``SWEEP_SMALL`` / ``SWEEP_LARGE`` name the single-product workloads: the
-  60,000-limb product and the size sweep with random, all-0xFFFFFFFF and 1:8
-  unbalanced operands.
+* ``SWEEP_SMALL`` / ``SWEEP_LARGE`` / ``SWEEP_ODD`` / ``SWEEP_XL`` name the
+  single-product workloads: the 60,000-limb product and the size sweep over
+  every power of two from 2^12 to 2^27 limbs, each with random,
+  all-0xFFFFFFFF and 1:8 unbalanced operands.
 """
 from __future__ import annotations
 
@@ -87,3 +88,7 @@ def _sweep(logs, seed0):
 C1 = {"name": "c1_60000", "na": 60000, "nb": 60000, "seed_a": 1, "seed_b": 2, "kind_a": 0, "kind_b": 0}
 SWEEP_SMALL = [C1] + _sweep([12, 14, 16, 18, 20], 1000)
 SWEEP_LARGE = _sweep([22, 24], 1000)
+# The odd powers between (2^17 .. 2^23 limbs) and the top of the sweep
+# (2^25 .. 2^27 limbs: transforms of 2^27 .. 2^29 points).
+SWEEP_ODD = _sweep([17, 19, 21, 23], 1000)
+SWEEP_XL = _sweep([25, 26, 27], 1000)

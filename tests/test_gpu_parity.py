@@ -60,7 +60,18 @@ def test_sweep_against_reference_hashes(b2m_gpu, entry):
     assert p.size == entry["len"] and sha_limbs(p) == entry["sha256"]
 
 
-@pytest.mark.parametrize("entry", (load("sweep_large.json") or {"products": []})["products"],
+def _sweep_entries(*names):
+    out = []
+    for nm in names:
+        out += (load(nm) or {"products": []})["products"]
+    return out
+
+
+# Every power of two from 2^17 to 2^27 limbs (transforms of 2^19 .. 2^29
+# points: two- and three-pass plans, the largest the default sweep reaches),
+# random, all-0xFFFFFFFF and 1:8 unbalanced, against the reference's own
+# mul_ntt_cpu hashes.
+@pytest.mark.parametrize("entry", _sweep_entries("sweep_odd.json", "sweep_large.json", "sweep_xl.json"),
                          ids=lambda e: e["name"])
 def test_large_sweep_against_reference_hashes(b2m_gpu, entry):
     a = gen_operand(entry["seed_a"], entry["na"], entry["kind_a"])

@@ -2,14 +2,16 @@
 allocate device memory when they multiply (their HBM belongs to another
 allocator, or cudaMalloc's synchronisation is not acceptable in their loop).
 
-It must give the same products as b2m_mul_device, on two calls in a row
-(the shared static scratch keeps the previous call's contents, so the second
-call checks that nothing stale leaks through), and reject sizes beyond its
-fixed limit of na + nb <= 2^19 limbs. This file is named to be collected last.
+It must give the same products as b2m_mul_device and as the oracle (the
+C restatement of the reference's CPU NTT), on two calls in a row (the shared
+static scratch keeps the previous call's contents, so the second call checks
+that nothing stale leaks through), and reject sizes beyond its fixed limit of
+na + nb <= 2^19 limbs. This file is named to be collected last.
 """
 import numpy as np
 import pytest
 
+import oracle
 from golden_util import gen_operand
 
 pytestmark = pytest.mark.gpu
@@ -34,6 +36,8 @@ def test_no_alloc_matches_pool_entry_point_twice(b2m_gpu, na, nb, kind):
     a_t = torch.from_numpy(a.view(np.int32)).cuda()
     b_t = torch.from_numpy(b.view(np.int32)).cuda()
     want = _product(b2m_gpu, torch, b2m_gpu.mul_device, a_t, na, b_t, nb)
+    ref = oracle.mul_port(a, b)
+    assert want.size == ref.size and np.array_equal(want, ref)
     for _ in range(2):
         got = _product(b2m_gpu, torch, b2m_gpu.mul_device_noalloc, a_t, na, b_t, nb)
         assert got.size == want.size and np.array_equal(got, want)
