@@ -43,20 +43,23 @@ GL_FN u64 gl_mulhi(u64 a, u64 b) {
 
 // a - b for a < 2^64, b <= p: a borrow wraps by 2^64 == EPS too many, and
 // since b - a <= p the corrected value cannot borrow again. Canonical when
-// a is. The device version is one 32-bit borrow chain: the borrow itself,
-// materialised as 0 or 0xFFFFFFFF (= EPS), is what gets subtracted.
+// a is. The device version is one 32-bit borrow chain plus the borrow bit
+// beta, and the correction d - beta*EPS = d + beta - beta*2^32 is done by a
+// wide multiply-add and a multiply-add on the high word: the integer ALU
+// pipe (which bounds the transforms) issues three instructions, the
+// otherwise idle FMA pipe the rest.
 GL_FN u64 gl_sub(u64 a, u64 b) {
 #if defined(__CUDA_ARCH__)
-    u32 d0, d1;
-    asm("{\n\t.reg .u32 m;\n\t"
-        "sub.cc.u32 %0, %2, %4;\n\t"
-        "subc.cc.u32 %1, %3, %5;\n\t"
-        "subc.u32 m, 0, 0;\n\t"
-        "sub.cc.u32 %0, %0, m;\n\t"
-        "subc.u32 %1, %1, 0;\n\t}"
-        : "=r"(d0), "=r"(d1)
+    u32 d0, d1, bt;
+    asm("sub.cc.u32 %0, %3, %5;\n\t"
+        "subc.cc.u32 %1, %4, %6;\n\t"
+        "subc.u32 %2, 0, 0;"
+        : "=r"(d0), "=r"(d1), "=r"(bt)
         : "r"((u32)a), "r"((u32)(a >> 32)), "r"((u32)b), "r"((u32)(b >> 32)));
-    return ((u64)d1 << 32) | d0;
+    // bt = -beta (0 or 0xFFFFFFFF)
+    u64 r;
+    asm("mad.wide.u32 %0, %1, 1, %2;" : "=l"(r) : "r"(0u - bt), "l"(((u64)d1 << 32) | d0));
+    return ((u64)((u32)(r >> 32) + bt) << 32) | (u32)r;
 #else
     u64 d = a - b;
     return (a < b) ? d - GL_EPS : d;
@@ -64,8 +67,8 @@ GL_FN u64 gl_sub(u64 a, u64 b) {
 }
 
 // a + b for canonical a, b, computed as a - (p - b) (p - b <= p, so gl_sub
-// applies): two instructions for p - b and the borrow chain of gl_sub,
-// instead of an add followed by two range checks.
+// applies): two instructions for p - b and gl_sub, instead of an add
+// followed by two range checks.
 GL_FN u64 gl_add(u64 a, u64 b) {
 #if defined(__CUDA_ARCH__)
     u32 n0, n1;
@@ -165,41 +168,69 @@ GL_FN u64 gl_mul(u64 a, u64 b) {
 #endif
 }
 
+#if defined(__CUDA_ARCH__)
+// x * 2^t for x < 2^64 and 0 < t < 32, canonical: x*2^t = W2*2^64 + L
+// (L = W1:W0, W2 < 2^t), and W2*2^64 == W2*EPS, so U = L + W2*EPS < 2p. One
+// wide multiply-add forms U mod 2^64 = T; U overflowed 2^64 exactly when
+// T < L (the added W2*EPS < 2^64). The canonical value is T + EPS (mod
+// 2^64) when U overflowed (then U - p = T + EPS, no wrap since T < 2^63) or
+// when T >= p (T + EPS carries), and T otherwise.
+__device__ __forceinline__ u64 gl_shl_w0(u64 x, int t) {
+    const u32 x0 = (u32)x, x1 = (u32)(x >> 32);
+    const u64 L = ((u64)__funnelshift_l(x0, x1, t) << 32) | (x0 << t);
+    const u32 W2 = x1 >> (32 - t);
+    u64 T;
+    asm("mad.wide.u32 %0, %1, -1, %2;" : "=l"(T) : "r"(W2), "l"(L));
+    u32 e0, e1, c;
+    asm("add.cc.u32 %0, %3, -1;\n\taddc.cc.u32 %1, %4, 0;\n\taddc.u32 %2, 0, 0;"
+        : "=r"(e0), "=r"(e1), "=r"(c)
+        : "r"((u32)T), "r"((u32)(T >> 32)));
+    return ((T < L) | c) ? (((u64)e1 << 32) | e0) : T;
+}
+
+// x * 2^(32 + t) for x < 2^64 and 0 <= t < 32, canonical: with W = x*2^t =
+// W2:W1:W0, x*2^(32+t) = W0*2^32 + W1*2^64 + W2*2^96 == (W0 + W1)*2^32 -
+// (W1 + W2). Writing W0 + W1 = hc*2^32 + h (hc*2^64 == hc*EPS), the first
+// term is A = (h + hc)*2^32 - hc, the 64-bit word pair (h, -hc) -- at most
+// p - 1, since hc = 1 forces h <= 2^32 - 2 -- and the second B = W1 + W2 <
+// 2^33, so the value is gl_sub(A, B), canonical.
+__device__ __forceinline__ u64 gl_shl_w1(u64 x, int t) {
+    const u32 x0 = (u32)x, x1 = (u32)(x >> 32);
+    const u32 W0 = x0 << t, W1 = t ? __funnelshift_l(x0, x1, t) : x1, W2 = t ? x1 >> (32 - t) : 0u;
+    u32 h, hc;
+    asm("add.cc.u32 %0, %2, %3;\n\taddc.u32 %1, 0, 0;" : "=r"(h), "=r"(hc) : "r"(W0), "r"(W1));
+    return gl_sub(((u64)h << 32) | (0u - hc), (u64)W1 + W2);
+}
+
+// x * 2^(64 + t) for x < 2^64 and 0 <= t < 32, canonical: W0*2^64 + W1*2^96
+// + W2*2^128 == W0*EPS - W1 - W2*2^32 = W0*2^32 - ((W2 + c)*2^32 + l) where
+// c:l = W0 + W1; the subtrahend is below 2^(32+t) + 2^33 <= p and the
+// minuend at most p - 1, so gl_sub gives the canonical value.
+__device__ __forceinline__ u64 gl_shl_w2(u64 x, int t) {
+    const u32 x0 = (u32)x, x1 = (u32)(x >> 32);
+    const u32 W0 = x0 << t, W1 = t ? __funnelshift_l(x0, x1, t) : x1, W2 = t ? x1 >> (32 - t) : 0u;
+    u32 l, c;
+    asm("add.cc.u32 %0, %2, %3;\n\taddc.u32 %1, 0, 0;" : "=r"(l), "=r"(c) : "r"(W0), "r"(W1));
+    return gl_sub((u64)W0 << 32, ((u64)(W2 + c) << 32) | l);
+}
+#endif
+
 // x * 2^s for canonical x and 0 <= s < 192. Written so that, with s known at
 // compile time (the register butterflies), every branch folds away; with s
 // warp-uniform at run time the branches are uniform.
 //
-// Device: s = 96n + 32w + t (n, w, t digits). x*2^t = W2:W1:W0 (W2 < 2^t) from
-// two 32-bit multiply-adds, then per word offset w:
-//   w = 0:  V == (W1 + W2)*2^32 + W0 - W2
-//   w = 1:  V == (W0 + W1)*2^32 - (W1 + W2)          (no range check needed)
-//   w = 2:  V == W0*2^32 - ((W2 + c)*2^32 + lo(W0 + W1)), c its carry
-// each an end-around carry plus one borrow chain (gl_hpl); 2^96 == -1 negates.
+// Device: s = 96n + 32w + t; the word offset w selects gl_shl_w0/w1/w2
+// (each canonical for any 64-bit input), and 2^96 == -1 negates.
 GL_FN u64 gl_shl(u64 x, int s) {
 #if defined(__CUDA_ARCH__)
     if (s == 0) return x;
     const bool neg = s >= 96;
     if (neg) s -= 96;
     const int t = s & 31, w = s >> 5;
-    u64 u, v;
-    asm("mul.wide.u32 %0, %1, %2;" : "=l"(u) : "r"((u32)x), "r"(1u << t));
-    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(v) : "r"((u32)(x >> 32)), "r"(1u << t), "l"(u >> 32));
-    const u32 W0 = (u32)u, W1 = (u32)v, W2 = (u32)(v >> 32);
     u64 r;
-    if (w == 0) {
-        u32 hc;
-        const u32 h = gl_ea_add(W1, W2, hc);
-        r = gl_canon(gl_hpl(h, W0, 0, W2 + hc));
-    } else if (w == 1) {
-        u32 hc, lc, ll;
-        const u32 h = gl_ea_add(W0, W1, hc);
-        gl_add3(W1, W2, hc, lc, ll);
-        r = gl_hpl(h, 0, lc, ll);
-    } else {
-        u32 c, ll;
-        asm("add.cc.u32 %0, %2, %3;\n\taddc.u32 %1, 0, 0;" : "=r"(ll), "=r"(c) : "r"(W0), "r"(W1));
-        r = gl_hpl(W0, 0, W2 + c, ll);
-    }
+    if (w == 0) r = t ? gl_shl_w0(x, t) : x;
+    else if (w == 1) r = gl_shl_w1(x, t);
+    else r = gl_shl_w2(x, t);
     return neg ? gl_sub(0, r) : r;
 #else
     bool neg = false;
