@@ -315,6 +315,27 @@ def run_ours(args) -> None:
     if not np.array_equal(dev, res):
         raise RuntimeError("device-resident and host-buffer products differ")
 
+    # The other two workloads the metric names, on the same GPUs: the batch of
+    # 4096 uneven products against one call per product, and the serving loop
+    # at the configured Poisson rate (every rank takes the same steps).
+    batch = serve = None
+    if not args.no_extra:
+        b = measure_batch(rk, args)
+        batch = {"workload": b["config"]["workload"], "jobs_per_gpu": b["config"]["jobs_rank0"],
+                 "glimbs_per_s": b["value"], "ms": b["ms_per_step"],
+                 "one_at_a_time_glimbs_per_s": b["one_at_a_time"]["value"],
+                 "one_at_a_time_ms": b["one_at_a_time"]["ms"],
+                 "speedup_vs_one_at_a_time": b["speedup_vs_one_at_a_time"],
+                 "bit_exact_vs_one_at_a_time": b["bit_exact_vs_one_at_a_time"]}
+        v = measure_serve(rk, args)
+        serve = {"workload": v["config"]["workload"], "requests": v["config"]["requests"],
+                 "p50_ms": v["value"], "p99_ms": v["p99_ms"], "mean_ms": v["mean_ms"],
+                 "served_glimbs_per_s": v["throughput"]["glimbs_per_s"],
+                 "offered_glimbs_per_s": v["throughput"]["offered_glimbs_per_s"],
+                 "max_queue": v["server"]["max_queue"],
+                 "max_inflight_dispatches": v["server"].get("max_inflight_dispatches"),
+                 "all_products_residue_checked_ok": v["all_products_residue_checked_ok"]}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_sample_log)
@@ -355,6 +376,8 @@ def run_ours(args) -> None:
                     "path": "b2m_mul_host (C ABI), pinned host buffers, wall clock per call"},
             "gpu_launches": plan["launches"] * args.steps,
             "clocks": clocks,
+            "batch": batch,
+            "serve": serve,
         }
         print(json.dumps(line), flush=True)
     ranks.close(rk)
@@ -373,16 +396,30 @@ def batch_sizes(n: int, seed: int):
 def run_batch(args) -> None:
     """Batched uneven products: 4096 log-uniform pairs in one graph launch
     versus one b2m_mul_device call per product on the same GPU."""
-    import numpy as np
     import torch
 
     import b200mul
     import ranks
 
     rk = ranks.from_env("nccl", timeout_s=300)
+    torch.cuda.set_device(rk.local)
+    b200mul.init(rk.local)
+    line = measure_batch(rk, args)
+    if rk.rank == 0:
+        print(json.dumps(line), flush=True)
+    ranks.close(rk)
+
+
+def measure_batch(rk, args) -> dict:
+    """The batch workload's JSON object (rank 0's is complete; the step times
+    are maxima over ranks)."""
+    import numpy as np
+    import torch
+
+    import b200mul
+    import ranks
+
     rank, world, local = rk.rank, rk.world, rk.local
-    torch.cuda.set_device(local)
-    b200mul.init(local)
     if args.batch_split and world > 1:
         # one batch of 4096 pairs, partitioned over the ranks by cost (LPT)
         everything = batch_sizes(args.batch_jobs, 4096)
@@ -450,28 +487,26 @@ def run_batch(args) -> None:
         raise RuntimeError("batched and one-at-a-time products differ")
     if world > 1:
         batched_ms, single_ms = ranks.max_over_ranks(rk, batched_ms, single_ms)
-    if rank == 0:
-        gl_b = job_limbs / (batched_ms * 1e-3) / 1e9
-        gl_s = job_limbs / (single_ms * 1e-3) / 1e9
-        print(json.dumps({
-            "metric": "batched Glimbs/s (4096 log-uniform pairs, 64..65536 limbs)", "value": round(gl_b, 3),
-            "unit": "Glimbs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(batched_ms, 4), "higher_is_better": True,
-            "scaling": "strong" if (args.batch_split and world > 1) else "weak",
-            "vs_baseline": None, "dtype": "u64 (GF(p), p=2^64-2^32+1)",
-            "data": "synthetic: seeded uniform random u32 limbs; lengths floor(2^(6+10u)), u uniform",
-            "config": {"workload": "4096 independent products, na and nb log-uniform in [64, 65536] limbs",
-                       "parallelism": ("one batch partitioned over the ranks by cost (LPT)"
-                                       if (args.batch_split and world > 1) else "one batch per rank"),
-                       "jobs_rank0": len(sizes), "input_limbs_all_ranks": job_limbs,
-                       "batch": "one CUDA-graph launch per step, size-bucketed, autotuned plans",
-                       "plan_and_autotune_s": round(plan_s, 2)},
-            "one_at_a_time": {"value": round(gl_s, 3), "unit": "Glimbs/s", "ms": round(single_ms, 3),
-                              "path": "one b2m_mul_device call per product on the same stream"},
-            "speedup_vs_one_at_a_time": round(single_ms / batched_ms, 2),
-            "bit_exact_vs_one_at_a_time": same,
-            "clocks": clocks}), flush=True)
-    ranks.close(rk)
+    gl_b = job_limbs / (batched_ms * 1e-3) / 1e9
+    gl_s = job_limbs / (single_ms * 1e-3) / 1e9
+    return {
+        "metric": "batched Glimbs/s (4096 log-uniform pairs, 64..65536 limbs)", "value": round(gl_b, 3),
+        "unit": "Glimbs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(batched_ms, 4), "higher_is_better": True,
+        "scaling": "strong" if (args.batch_split and world > 1) else "weak",
+        "vs_baseline": None, "dtype": "u64 (GF(p), p=2^64-2^32+1)",
+        "data": "synthetic: seeded uniform random u32 limbs; lengths floor(2^(6+10u)), u uniform",
+        "config": {"workload": "4096 independent products, na and nb log-uniform in [64, 65536] limbs",
+                   "parallelism": ("one batch partitioned over the ranks by cost (LPT)"
+                                   if (args.batch_split and world > 1) else "one batch per rank"),
+                   "jobs_rank0": len(sizes), "input_limbs_all_ranks": job_limbs,
+                   "batch": "one CUDA-graph launch per step, size-bucketed, autotuned plans",
+                   "plan_and_autotune_s": round(plan_s, 2)},
+        "one_at_a_time": {"value": round(gl_s, 3), "unit": "Glimbs/s", "ms": round(single_ms, 3),
+                          "path": "one b2m_mul_device call per product on the same stream"},
+        "speedup_vs_one_at_a_time": round(single_ms / batched_ms, 2),
+        "bit_exact_vs_one_at_a_time": same,
+        "clocks": clocks}
 
 
 def run_chudnovsky(args) -> None:
@@ -649,22 +684,33 @@ def run_serve(args) -> None:
     lengths log-uniform in [2^10, 2^24] limbs, seeded operands generated on
     the device, continuous batching under an HBM budget; p50/p99 latency and
     throughput, every product residue-checked on the device."""
-    import numpy as np
     import torch
 
     import b200mul
-
     import ranks
 
     # Several GPUs: one server per rank, each with its own arrival stream at
     # --rate (weak scaling); latencies and throughput gathered to rank 0.
     rk = ranks.from_env("nccl", timeout_s=600)
+    torch.cuda.set_device(rk.local)
+    b200mul.init(rk.local)
+    line = measure_serve(rk, args)
+    ranks.close(rk)
+    if rk.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def measure_serve(rk, args, rate: float | None = None) -> dict:
+    """The serving workload's JSON object at `rate` req/s (default --rate)."""
+    import numpy as np
+
+    import b200mul
+
     rank, local = rk.rank, rk.local
-    torch.cuda.set_device(local)
-    b200mul.init(local)
+    rate = args.rate if rate is None else rate
     rng = np.random.default_rng(2000 + rank)
-    n_req = int(args.rate * args.duration)
-    gaps = rng.exponential(1.0 / args.rate, n_req)
+    n_req = int(rate * args.duration)
+    gaps = rng.exponential(1.0 / rate, n_req)
     arrivals = np.cumsum(gaps)
     lens = (2.0 ** rng.uniform(10, 24, (n_req, 2))).astype(np.int64)
     srv = b200mul.Server(hbm_budget_bytes=args.serve_budget_gb << 30, streams=args.serve_streams,
@@ -722,24 +768,22 @@ def run_serve(args) -> None:
         offered_limbs = sum(e["offered"] for e in every)
         wall = max(e["wall"] for e in every)
         n_req = sum(e["n"] for e in every)
-    ranks.close(rk)
     lat = np.array(lat)
-    if rank == 0:
-        print(json.dumps({
-            "metric": "serve p50/p99 latency ms (Poisson arrivals, log-uniform 2^10..2^24 limbs)",
-            "value": round(float(np.percentile(lat, 50)), 2), "unit": "ms",
-            "p99_ms": round(float(np.percentile(lat, 99)), 2), "mean_ms": round(float(lat.mean()), 2),
-            "n_gpus": rk.world, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u64 (GF(p), p=2^64-2^32+1)",
-            "data": "synthetic: seeded random limbs generated on the device per request",
-            "config": {"workload": f"{args.rate} req/s Poisson for {args.duration} s per GPU", "requests": n_req,
-                       "hbm_budget_gb": args.serve_budget_gb, "streams": args.serve_streams,
-                       "max_batch": args.serve_batch, "submit_window_s": round(submit_end, 2)},
-            "throughput": {"req_per_s": round(n_req / wall, 1), "glimbs_per_s": round(limbs_done / wall / 1e9, 3),
-                           "offered_glimbs_per_s": round(offered_limbs / args.duration / 1e9, 3),
-                           "wall_s": round(wall, 2)},
-            "all_products_residue_checked_ok": bad == 0, "failed_or_mismatched": bad,
-            "server": st, "clocks": clocks}), flush=True)
+    return {
+        "metric": "serve p50/p99 latency ms (Poisson arrivals, log-uniform 2^10..2^24 limbs)",
+        "value": round(float(np.percentile(lat, 50)), 2), "unit": "ms",
+        "p99_ms": round(float(np.percentile(lat, 99)), 2), "mean_ms": round(float(lat.mean()), 2),
+        "n_gpus": rk.world, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u64 (GF(p), p=2^64-2^32+1)",
+        "data": "synthetic: seeded random limbs generated on the device per request",
+        "config": {"workload": f"{rate} req/s Poisson for {args.duration} s per GPU", "requests": n_req,
+                   "hbm_budget_gb": args.serve_budget_gb, "streams": args.serve_streams,
+                   "max_batch": args.serve_batch, "submit_window_s": round(submit_end, 2)},
+        "throughput": {"req_per_s": round(n_req / wall, 1), "glimbs_per_s": round(limbs_done / wall / 1e9, 3),
+                       "offered_glimbs_per_s": round(offered_limbs / args.duration / 1e9, 3),
+                       "wall_s": round(wall, 2)},
+        "all_products_residue_checked_ok": bad == 0, "failed_or_mismatched": bad,
+        "server": st, "clocks": clocks}
 
 
 def main():
@@ -768,6 +812,8 @@ def main():
     ap.add_argument("--cpu-sample-log", type=int, default=24,
                     help="log2 limbs of the CPU-baseline product (24: the headline product itself)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="single: skip the batch and serving measurements that the default line carries")
     ap.add_argument("--autotune", action="store_true",
                     help="single: time every candidate plan first and keep the fastest (the default plan of each "
                          "length is already the measured fastest; candidates within noise of it may win)")

@@ -359,6 +359,7 @@ static void scheduler(b2m_server* S) {
             for (size_t k = 0; k < order.size(); ++k) sl.ids[k] = ids[order[k]];
             sl.busy = true;
             ++S->st.inflight_dispatches;
+            S->st.max_inflight_dispatches = std::max(S->st.max_inflight_dispatches, S->st.inflight_dispatches);
             ++S->st.dispatches;
             progressed = true;
         }

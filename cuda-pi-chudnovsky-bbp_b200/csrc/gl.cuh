@@ -213,6 +213,7 @@ __device__ __forceinline__ u64 gl_shl_w2(u64 x, int t) {
     asm("add.cc.u32 %0, %2, %3;\n\taddc.u32 %1, 0, 0;" : "=r"(l), "=r"(c) : "r"(W0), "r"(W1));
     return gl_sub((u64)W0 << 32, ((u64)(W2 + c) << 32) | l);
 }
+
 #endif
 
 // x * 2^s for canonical x and 0 <= s < 192. Written so that, with s known at
@@ -251,6 +252,43 @@ GL_FN u64 gl_shl(u64 x, int s) {
         r = gl_sub(gl_reduce128(0, zl), zh << 32);
     }
     return neg ? gl_neg(r) : r;
+#endif
+}
+
+// x * 2^s for x < 2^64 and a run-time, warp-uniform 0 <= s < 192: one copy
+// of the three word-offset folds behind uniform branches (t = 0 needs no
+// case of its own: the funnel shifts give W2 = 0 and the folds stay exact),
+// so a site costs a few hundred bytes of code instead of one specialised
+// body per shift amount.
+static __device__ __noinline__ u64 gl_shl_rt(u64 x, u32 s) {
+#if defined(__CUDA_ARCH__)
+    const bool neg = s >= 96;
+    if (neg) s -= 96;
+    const u32 t = s & 31, w = s >> 5;
+    const u32 x0 = (u32)x, x1 = (u32)(x >> 32);
+    const u32 W0 = x0 << t, W1 = __funnelshift_l(x0, x1, t), W2 = __funnelshift_l(x1, 0u, t);
+    u64 r;
+    if (w == 0) {
+        const u64 L = ((u64)W1 << 32) | W0;
+        u64 T;
+        asm("mad.wide.u32 %0, %1, -1, %2;" : "=l"(T) : "r"(W2), "l"(L));
+        u32 e0, e1, c;
+        asm("add.cc.u32 %0, %3, -1;\n\taddc.cc.u32 %1, %4, 0;\n\taddc.u32 %2, 0, 0;"
+            : "=r"(e0), "=r"(e1), "=r"(c)
+            : "r"((u32)T), "r"((u32)(T >> 32)));
+        r = ((T < L) | c) ? (((u64)e1 << 32) | e0) : T;
+    } else if (w == 1) {
+        u32 h, hc;
+        asm("add.cc.u32 %0, %2, %3;\n\taddc.u32 %1, 0, 0;" : "=r"(h), "=r"(hc) : "r"(W0), "r"(W1));
+        r = gl_sub(((u64)h << 32) | (0u - hc), (u64)W1 + W2);
+    } else {
+        u32 l, c;
+        asm("add.cc.u32 %0, %2, %3;\n\taddc.u32 %1, 0, 0;" : "=r"(l), "=r"(c) : "r"(W0), "r"(W1));
+        r = gl_sub((u64)W0 << 32, ((u64)(W2 + c) << 32) | l);
+    }
+    return neg ? gl_sub(0, r) : r;
+#else
+    return gl_shl(x, (int)s);
 #endif
 }
 

@@ -197,19 +197,34 @@ __device__ __forceinline__ void level1_twiddle(u64* x) {
     }
 }
 
-// The same for a warp-uniform run-time u1 in [0, 8): one uniform branch to
-// the compile-time form.
-template <bool INV>
+// The same for a warp-uniform run-time u1 in [0, 8), two ways:
+//  RT = false: one uniform branch to the compile-time form (eight specialised
+//    bodies per direction; fastest where a kernel holds one direction);
+//  RT = true: shift amounts 3 * u1 * k1 (mod 192) formed at run time and one
+//    out-of-line run-time shift routine, so the kernel carries one copy of the
+//    code -- the fused pass (both directions in one kernel) was bound by
+//    instruction fetch with the specialised bodies, and the inverse passes
+//    measured faster this way too.
+template <bool INV, bool RT>
 __device__ __forceinline__ void level1_twiddle(u64* x, int u1) {
-    switch (u1) {
-        case 0: break;
-        case 1: level1_twiddle<1, INV>(x); break;
-        case 2: level1_twiddle<2, INV>(x); break;
-        case 3: level1_twiddle<3, INV>(x); break;
-        case 4: level1_twiddle<4, INV>(x); break;
-        case 5: level1_twiddle<5, INV>(x); break;
-        case 6: level1_twiddle<6, INV>(x); break;
-        default: level1_twiddle<7, INV>(x); break;
+    if constexpr (RT) {
+        if (u1 == 0) return;
+#pragma unroll
+        for (int i = 1; i < 8; ++i) {
+            const u32 s = (u32)(3 * brev_c(i, 3)) * (u32)u1;  // < 192
+            x[i] = gl_shl_rt(x[i], INV ? 192u - s : s);
+        }
+    } else {
+        switch (u1) {
+            case 0: break;
+            case 1: level1_twiddle<1, INV>(x); break;
+            case 2: level1_twiddle<2, INV>(x); break;
+            case 3: level1_twiddle<3, INV>(x); break;
+            case 4: level1_twiddle<4, INV>(x); break;
+            case 5: level1_twiddle<5, INV>(x); break;
+            case 6: level1_twiddle<6, INV>(x); break;
+            default: level1_twiddle<7, INV>(x); break;
+        }
     }
 }
 
@@ -224,7 +239,7 @@ __device__ __forceinline__ void level1_twiddle(u64* x, int u1) {
 // Task order puts the level index (u1 or i1) outermost so it is uniform
 // across a warp whenever the tile has >= 32 instances.
 // ---------------------------------------------------------------------------
-template <class TL, int LOGL, bool INV>
+template <class TL, int LOGL, bool INV, bool RT>
 __device__ __forceinline__ void group64(u64* sm, const u64* __restrict__ dtw) {
     constexpr int L = 1 << LOGL, LOGJ = LOGL - 6, JW = 1 << LOGJ;
     constexpr int LOGNI = TL::LR - 6 + TL::LC;  // instances = C * R / 64
@@ -242,9 +257,9 @@ __device__ __forceinline__ void group64(u64* sm, const u64* __restrict__ dtw) {
             for (int m = 0; m < 8; ++m) x[m] = ptr[m * st];
             if (!INV) {
                 dft_fwd<8>(x);
-                level1_twiddle<false>(x, u1);
+                level1_twiddle<false, RT>(x, u1);
             } else {
-                level1_twiddle<true>(x, u1);
+                level1_twiddle<true, RT>(x, u1);
                 dft_inv<8>(x);
             }
 #pragma unroll
@@ -322,48 +337,49 @@ __device__ __forceinline__ void lone8(u64* sm) {
 }
 
 // Radix-64 groups from block size 2^LOGL down, G groups.
-template <class TL, int LOGL, int G>
+template <class TL, int LOGL, int G, bool RT>
 __device__ __forceinline__ void groups_fwd(u64* sm, const u64* dtw) {
     if constexpr (G > 0) {
-        group64<TL, LOGL, false>(sm, dtw);
+        group64<TL, LOGL, false, RT>(sm, dtw);
         __syncthreads();
-        groups_fwd<TL, LOGL - 6, G - 1>(sm, dtw);
+        groups_fwd<TL, LOGL - 6, G - 1, RT>(sm, dtw);
     }
 }
-template <class TL, int LOGL, int G>
+template <class TL, int LOGL, int G, bool RT>
 __device__ __forceinline__ void groups_inv(u64* sm, const u64* dtw) {
     // inverse order: smallest block first
     if constexpr (G > 0) {
-        groups_inv<TL, LOGL - 6, G - 1>(sm, dtw);
-        group64<TL, LOGL, true>(sm, dtw);
+        groups_inv<TL, LOGL - 6, G - 1, RT>(sm, dtw);
+        group64<TL, LOGL, true, RT>(sm, dtw);
         __syncthreads();
     }
 }
 
 // Whole column DFTs of the tile held in shared memory (callers synchronise
-// before; the functions end with the tile synchronised).
-template <class TL>
+// before; the functions end with the tile synchronised). RT selects the form
+// of the level-1 twiddles (level1_twiddle above).
+template <class TL, bool RT = false>
 __device__ __forceinline__ void tile_fwd(u64* sm, const u64* dtw) {
     using S = Steps<TL::LR>;
     if constexpr (S::A > 0) {
         lead_step<TL, S::A, false>(sm, dtw);
         __syncthreads();
     }
-    groups_fwd<TL, TL::LR - S::A, S::G>(sm, dtw);
+    groups_fwd<TL, TL::LR - S::A, S::G, RT>(sm, dtw);
     if constexpr (S::LONE) {
         lone8<TL, false>(sm);
         __syncthreads();
     }
 }
 
-template <class TL>
+template <class TL, bool RT = true>
 __device__ __forceinline__ void tile_inv(u64* sm, const u64* dtw) {
     using S = Steps<TL::LR>;
     if constexpr (S::LONE) {
         lone8<TL, true>(sm);
         __syncthreads();
     }
-    groups_inv<TL, TL::LR - S::A, S::G>(sm, dtw);
+    groups_inv<TL, TL::LR - S::A, S::G, RT>(sm, dtw);
     if constexpr (S::A > 0) {
         lead_step<TL, S::A, true>(sm, dtw);
         __syncthreads();

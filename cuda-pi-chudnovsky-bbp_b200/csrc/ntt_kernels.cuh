@@ -262,7 +262,7 @@ k_fused_last(u64* __restrict__ bbuf, const u64* __restrict__ aspec, u64 ninv, Ro
     for (int k = 0; k < G::PER; ++k) cp_async8(sm + gp.sa0 + G::soff(k), base + k * TL::T);
     cp_async_wait_all();
     __syncthreads();
-    tile_fwd<TL>(sm, tw.dtw);
+    tile_fwd<TL, true>(sm, tw.dtw);
     if (square) {
 #pragma unroll
         for (int k = 0; k < G::PER; ++k) {

@@ -150,7 +150,8 @@ typedef enum b2m_field_op {
     B2M_FIELD_POW = 4,
     B2M_FIELD_INV = 5,
     B2M_FIELD_DFT8 = 6,
-    B2M_FIELD_IDFT8 = 7
+    B2M_FIELD_IDFT8 = 7,
+    B2M_FIELD_SHL_RT = 8  /* a * 2^(b mod 192) by the run-time shift of the level-1 twiddles */
 } b2m_field_op;
 b2m_status b2m_field_eval_host(int op, const uint64_t* a, const uint64_t* b, uint64_t* out, uint64_t n);
 
@@ -334,6 +335,7 @@ typedef struct b2m_server_stats {
     uint64_t submitted, completed, failed, dispatches;
     uint64_t inflight_dispatches, queued, max_queue;
     uint64_t bytes_in_use, peak_bytes;
+    uint64_t max_inflight_dispatches;  /* most dispatches on the GPU at one time */
 } b2m_server_stats;
 
 b2m_status b2m_server_start(const b2m_server_config* cfg, b2m_server** server);

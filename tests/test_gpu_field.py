@@ -63,8 +63,10 @@ def test_every_shift_amount(b2m_gpu):
     vals = EDGE + [int(v) % P for v in rng.integers(0, 2**63, 40, dtype=np.uint64)]
     xs = [x for x in vals for _ in range(192)]
     ss = [s for _ in vals for s in range(192)]
-    got = b2m_gpu.field_eval("shl", arr(xs), arr(ss))
-    assert ints(got) == [(x << s) % P for x, s in zip(xs, ss)]
+    want = [(x << s) % P for x, s in zip(xs, ss)]
+    assert ints(b2m_gpu.field_eval("shl", arr(xs), arr(ss))) == want
+    # the run-time (warp-uniform) shift of the level-1 twiddles
+    assert ints(b2m_gpu.field_eval("shl_rt", arr(xs), arr(ss))) == want
 
 
 def test_random_pairs(b2m_gpu):

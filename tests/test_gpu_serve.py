@@ -102,3 +102,43 @@ def test_caller_owned_buffers_and_stop_drains(b2m_gpu):
     want = b2m_gpu.mul_ntt_cuda(a, b)
     assert np.array_equal(got[: want.size], want)
     del t, extra
+
+
+def test_continuous_admission_while_dispatches_run(b2m_gpu):
+    """Continuous batching, not a queue alone: a second wave submitted while
+    the first wave's dispatches are on the GPU is admitted before the first
+    wave completes, dispatches run concurrently on the server's streams, and
+    every product of both waves is the same as alone."""
+    import time
+
+    torch = pytest.importorskip("torch")
+    srv = b2m_gpu.Server(hbm_budget_bytes=16 << 30, streams=4, max_batch=2)
+    big = 1 << 22  # each product ~1 ms of device time
+    wave1 = [(srv.submit(big, big, 300 + i, 400 + i), big, big, 300 + i, 400 + i) for i in range(8)]
+    # wait until the first wave is on the GPU (admitted, not yet done)
+    t0 = time.time()
+    while time.time() - t0 < 30:
+        states = [srv.poll(t).state for t, *_ in wave1]
+        if any(s >= 1 for s in states):
+            break
+        time.sleep(0.0002)
+    assert any(s >= 1 for s in states), states
+    wave2 = [(srv.submit(n, m, 500 + i, 600 + i), n, m, 500 + i, 600 + i)
+             for i, (n, m) in enumerate([(1 << 20, 1 << 20), (70000, 3000), (1 << 21, 1 << 19), (4096, 4096)])]
+    res1 = [srv.wait(t, 120.0) for t, *_ in wave1]
+    res2 = [srv.wait(t, 120.0) for t, *_ in wave2]
+    assert all(r.state == b2m_gpu.DONE and r.residues_ok == 1 for r in res1 + res2)
+    last_done_1 = max(r.t_done_ns for r in res1)
+    # some second-wave request was admitted to the GPU while the first wave ran
+    assert min(r.t_admit_ns for r in res2) < last_done_1
+    # admitted requests overlapped in time on the device (intervals [admit, done] intersect across dispatches)
+    spans = sorted((r.t_admit_ns, r.t_done_ns) for r in res1 + res2)
+    assert any(spans[i + 1][0] < spans[i][1] for i in range(len(spans) - 1))
+    st = srv.stats()
+    assert st["max_inflight_dispatches"] >= 2 and st["dispatches"] >= 5
+    for (t, na, nb, sa, sb), r in zip(wave1 + wave2, res1 + res2):
+        got = _copy_out(torch, r.out, r.out_len)
+        alone = b2m_gpu.mul_ntt_cuda(gen_operand(sa, na), gen_operand(sb, nb))
+        assert np.array_equal(got, alone), (na, nb)
+        srv.release(t)
+    srv.stop()
