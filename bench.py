@@ -327,14 +327,24 @@ def run_ours(args) -> None:
                  "one_at_a_time_ms": b["one_at_a_time"]["ms"],
                  "speedup_vs_one_at_a_time": b["speedup_vs_one_at_a_time"],
                  "bit_exact_vs_one_at_a_time": b["bit_exact_vs_one_at_a_time"]}
-        v = measure_serve(rk, args)
-        serve = {"workload": v["config"]["workload"], "requests": v["config"]["requests"],
-                 "p50_ms": v["value"], "p99_ms": v["p99_ms"], "mean_ms": v["mean_ms"],
-                 "served_glimbs_per_s": v["throughput"]["glimbs_per_s"],
-                 "offered_glimbs_per_s": v["throughput"]["offered_glimbs_per_s"],
-                 "max_queue": v["server"]["max_queue"],
-                 "max_inflight_dispatches": v["server"].get("max_inflight_dispatches"),
-                 "all_products_residue_checked_ok": v["all_products_residue_checked_ok"]}
+        def summary(v):
+            return {"workload": v["config"]["workload"], "requests": v["config"]["requests"],
+                    "p50_ms": v["value"], "p99_ms": v["p99_ms"], "mean_ms": v["mean_ms"],
+                    "served_glimbs_per_s": v["throughput"]["glimbs_per_s"],
+                    "offered_glimbs_per_s": v["throughput"]["offered_glimbs_per_s"],
+                    "max_queue": v["server"]["max_queue"],
+                    "max_inflight_dispatches": v["server"].get("max_inflight_dispatches"),
+                    "all_products_residue_checked_ok": v["all_products_residue_checked_ok"]}
+
+        at_cfg = summary(measure_serve(rk, args))
+        serve = {"at_config_rate": at_cfg}
+        # A sustainable rate: when the configured rate overloads the server
+        # (its queue grows), 90% of the rate it actually served; otherwise the
+        # configured rate itself is sustainable and is not repeated.
+        ratio = at_cfg["served_glimbs_per_s"] / max(at_cfg["offered_glimbs_per_s"], 1e-9)
+        if ratio < 0.97:
+            sus_rate = round(0.9 * ratio * args.rate, 1)
+            serve["at_sustainable_rate"] = summary(measure_serve(rk, args, rate=sus_rate))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -698,6 +708,39 @@ def run_serve(args) -> None:
     ranks.close(rk)
     if rk.rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def serve_capacity(rk, args, n_req: int = 600) -> dict:
+    """Closed-loop capacity of the server on the serving size mix: n_req
+    requests (lengths log-uniform in [2^10, 2^24] limbs) submitted at once,
+    time to complete them all (max over ranks)."""
+    import numpy as np
+
+    import b200mul
+    import ranks
+
+    rng = np.random.default_rng(3000 + rk.rank)
+    lens = (2.0 ** rng.uniform(10, 24, (n_req, 2))).astype(np.int64)
+    srv = b200mul.Server(hbm_budget_bytes=args.serve_budget_gb << 30, streams=args.serve_streams,
+                         max_batch=args.serve_batch)
+    warm = [srv.submit(1 << k, 1 << k, 99 + k, 199 + k) for k in range(10, 25)]
+    for t in warm:
+        srv.wait(t, 120.0)
+        srv.release(t)
+    t0 = time.perf_counter()
+    ts = [srv.submit(int(a), int(b), 11 * i + 3, 11 * i + 4) for i, (a, b) in enumerate(lens)]
+    bad = 0
+    for t in ts:
+        r = srv.wait(t, 300.0)
+        bad += int(r.state != b200mul.DONE or r.residues_ok != 1)
+        srv.release(t)
+    wall = time.perf_counter() - t0
+    srv.stop()
+    wall = ranks.max_over_ranks(rk, wall)
+    limbs = int(lens.sum()) * rk.world
+    return {"requests": n_req * rk.world, "wall_s": round(wall, 3),
+            "glimbs_per_s": round(limbs / wall / 1e9, 3), "req_per_s": round(n_req * rk.world / wall, 1),
+            "mean_limbs_per_request": int(lens.sum()) // n_req, "all_ok": bad == 0}
 
 
 def measure_serve(rk, args, rate: float | None = None) -> dict:

@@ -513,7 +513,7 @@ class Result(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [(n, _u64) for n in ("submitted", "completed", "failed", "dispatches", "inflight_dispatches",
                                     "queued", "max_queue", "bytes_in_use", "peak_bytes",
-                                    "max_inflight_dispatches")]
+                                    "max_inflight_dispatches", "host_dispatch_ns", "slot_busy_ns")]
 
 
 _sig("b2m_server_start", ctypes.c_int, [ctypes.POINTER(ServerConfig), ctypes.POINTER(ctypes.c_void_p)])

@@ -120,6 +120,7 @@ struct Slot {
     uint64_t arena_cap = 0;
     void* host = nullptr;         // pinned: lengths + residues + error word
     uint64_t host_cap = 0;
+    uint64_t t_start = 0;         // when the running dispatch was enqueued
 };
 
 }  // namespace b2m
@@ -175,10 +176,12 @@ static cudaError_t launch_dispatch(b2m_server* S, Slot& sl, std::vector<Req>& rv
         }
     sl.block_bytes = tab + lens + res + bufs + scr;
     if (sl.block_bytes > sl.arena_cap) {
-        // grow by at least a quarter, in 256 MiB steps (the previous dispatch
-        // on this slot has completed, so its arena can go)
-        const uint64_t cap = al(std::max<uint64_t>(sl.block_bytes, sl.arena_cap + sl.arena_cap / 4) + (256ull << 20)) &
-                             ~((256ull << 20) - 1);
+        // grow to at least twice the old size (256 MiB granules; the previous
+        // dispatch on this slot has completed, so its arena can go): every
+        // growth maps fresh device memory, which costs the scheduler thread
+        // time proportional to its size, so growth steps must be few
+        const uint64_t gran = 256ull << 20;
+        const uint64_t cap = (std::max<uint64_t>(sl.block_bytes, 2 * sl.arena_cap) + gran - 1) & ~(gran - 1);
         if (sl.arena) {
             cudaFreeAsync(sl.arena, s);
             budget_release(S->c, sl.arena_cap);
@@ -302,6 +305,7 @@ static void scheduler(b2m_server* S) {
             }
             sl.busy = false;
             sl.ids.clear();
+            S->st.slot_busy_ns += t - sl.t_start;
             --S->st.inflight_dispatches;
             progressed = true;
             S->cv_done.notify_all();
@@ -328,7 +332,9 @@ static void scheduler(b2m_server* S) {
                 }
             }
             if (rs.empty()) break;
+            const uint64_t t_enq = now_ns();
             cudaError_t e = launch_dispatch(S, sl, rs);
+            const uint64_t t_enq_end = now_ns();
             std::lock_guard<std::mutex> lk(S->mu);
             for (size_t k = 0; k < rs.size(); ++k) {  // publish the owned buffers
                 Req& r = S->reqs[ids[k]];
@@ -358,6 +364,8 @@ static void scheduler(b2m_server* S) {
             sl.ids.resize(rs.size());
             for (size_t k = 0; k < order.size(); ++k) sl.ids[k] = ids[order[k]];
             sl.busy = true;
+            sl.t_start = t_enq;
+            S->st.host_dispatch_ns += t_enq_end - t_enq;
             ++S->st.inflight_dispatches;
             S->st.max_inflight_dispatches = std::max(S->st.max_inflight_dispatches, S->st.inflight_dispatches);
             ++S->st.dispatches;
@@ -402,6 +410,31 @@ b2m_status b2m_server_start(const b2m_server_config* cfg, b2m_server** out) {
         cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming);
     }
     cudaStreamCreateWithFlags(&S->release_stream, cudaStreamNonBlocking);
+    // Twiddle tables of every transform length the budget can admit, built
+    // now: building one later means a cudaMalloc (which synchronises the
+    // device) and a stream wait inside the scheduler, stalling every
+    // dispatch in flight.
+    for (int logn = SMALL_MAX_LOGN + 1; logn <= MAX_LOGN; ++logn) {
+        const uint64_t pts = 1ull << logn;
+        if (2 * 8 * pts > S->cfg.hbm_budget_bytes) break;
+        if (twtable_ensure(c, plan_for(c, logn), S->release_stream) != cudaSuccess) break;
+    }
+    // Each slot's arena starts at an equal share of half the budget (at most
+    // 4 GiB), so that typical dispatches never grow it.
+    {
+        const uint64_t gran = 256ull << 20;
+        uint64_t share = std::min<uint64_t>(S->cfg.hbm_budget_bytes / (2 * S->cfg.streams), 4ull << 30) & ~(gran - 1);
+        for (Slot& sl : S->slots) {
+            if (share == 0 || !budget_reserve(c, share)) break;
+            if (cudaMallocAsync(&sl.arena, share, sl.s) != cudaSuccess) {
+                budget_release(c, share);
+                sl.arena = nullptr;
+                cudaGetLastError();
+                break;
+            }
+            sl.arena_cap = share;
+        }
+    }
     S->th = std::thread(scheduler, S);
     *out = S;
     return B2M_OK;

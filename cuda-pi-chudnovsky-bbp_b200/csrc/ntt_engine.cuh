@@ -357,8 +357,11 @@ __device__ __forceinline__ void groups_inv(u64* sm, const u64* dtw) {
 
 // Whole column DFTs of the tile held in shared memory (callers synchronise
 // before; the functions end with the tile synchronised). RT selects the form
-// of the level-1 twiddles (level1_twiddle above).
-template <class TL, bool RT = false>
+// of the level-1 twiddles (level1_twiddle above): forward tiles with one
+// radix-64 group keep the specialised bodies, tiles with two groups (whose
+// specialised code stalled on instruction fetch) and all inverse tiles use
+// the run-time shifts.
+template <class TL, bool RT = (Steps<TL::LR>::G >= 2)>
 __device__ __forceinline__ void tile_fwd(u64* sm, const u64* dtw) {
     using S = Steps<TL::LR>;
     if constexpr (S::A > 0) {

@@ -336,6 +336,8 @@ typedef struct b2m_server_stats {
     uint64_t inflight_dispatches, queued, max_queue;
     uint64_t bytes_in_use, peak_bytes;
     uint64_t max_inflight_dispatches;  /* most dispatches on the GPU at one time */
+    uint64_t host_dispatch_ns;         /* scheduler time spent enqueueing dispatches */
+    uint64_t slot_busy_ns;             /* summed over slots: enqueue to observed completion */
 } b2m_server_stats;
 
 b2m_status b2m_server_start(const b2m_server_config* cfg, b2m_server** server);

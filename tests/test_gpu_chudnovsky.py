@@ -43,7 +43,7 @@ def test_tree_roots_match_reference(b2m_gpu, digits):
     r.free()
 
 
-@pytest.mark.parametrize("digits", [1000, 100000, 1000000])
+@pytest.mark.parametrize("digits", [1000, 100000, 1000000, 3000000])
 def test_compute_pi_matches_reference_digits(b2m_gpu, digits):
     runs = {r["digits"]: r for r in json.load(open(os.path.join(GOLD, "pi_digits.json")))["runs"]}
     if digits not in runs:
@@ -51,6 +51,17 @@ def test_compute_pi_matches_reference_digits(b2m_gpu, digits):
     s = b2m_gpu.compute_pi(digits)
     assert s[:102] == runs[digits]["head"]
     assert hashlib.sha256(s.encode()).hexdigest() == runs[digits]["sha256"]
+
+
+def test_ten_million_digit_string_prefix_matches_reference(b2m_gpu):
+    """The 10,000,000-digit string (the Chudnovsky config): its leading
+    3,000,000 digits equal the reference's own 3,000,000-digit run
+    (src/chudnovsky.cpp:107-164 via oracle/_ref, 4,220 s on one core)."""
+    runs = {r["digits"]: r for r in json.load(open(os.path.join(GOLD, "pi_digits.json")))["runs"]}
+    d = max(runs)
+    s = b2m_gpu.compute_pi(10000000)
+    assert len(s) == 10000002 and s[:102] == runs[d]["head"]
+    assert hashlib.sha256(s[: 2 + d].encode()).hexdigest() == runs[d]["sha256"]
 
 
 @pytest.mark.parametrize("digits", [1000, 100000, 1000000])
