@@ -81,7 +81,9 @@ __device__ __forceinline__ CState cs_shfl_up(CState s, int off) {
 
 // Block-wide exclusive scan of carry functions. Returns the thread's
 // exclusive prefix (valid only when *has_prefix), and the block aggregate in
-// *agg (all threads). `ws` needs one CState per warp plus one.
+// *agg (all threads). `ws` needs one CState per warp. One barrier: every warp
+// scans the warp aggregates itself with shuffles (no serial pass on one
+// thread, no second barrier); callers synchronise before writing `ws` again.
 __device__ __forceinline__ CState block_scan_carry(CState st, bool* has_prefix, CState* agg, CState* ws) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nwarps = (blockDim.x + 31) >> 5;
@@ -94,21 +96,23 @@ __device__ __forceinline__ CState block_scan_carry(CState st, bool* has_prefix, 
     CState exw = cs_shfl_up(inc, 1);
     if (lane == 31 || (int)threadIdx.x == (int)blockDim.x - 1) ws[warp] = inc;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        CState acc = ws[0];
-        for (int w = 1; w < nwarps; ++w) {
-            CState tw = ws[w];
-            ws[w] = acc;  // exclusive prefix of warp w
-            acc = cs_then(acc, tw);
-        }
-        ws[nwarps] = acc;
+    // inclusive scan of the warp aggregates, lanes [0, nwarps) meaningful
+    CState wv = ws[lane < nwarps ? lane : nwarps - 1];
+    for (int off = 1; off < nwarps; off <<= 1) {
+        CState o = cs_shfl_up(wv, off);
+        if (lane >= off) wv = cs_then(o, wv);
     }
-    __syncthreads();
-    *agg = ws[nwarps];
+    CState a;
+    a.h = __shfl_sync(0xFFFFFFFFu, wv.h, nwarps - 1);
+    a.t = __shfl_sync(0xFFFFFFFFu, wv.t, nwarps - 1);
+    *agg = a;
+    CState exb;  // inclusive aggregate of the warps before this one
+    exb.h = __shfl_sync(0xFFFFFFFFu, wv.h, warp > 0 ? warp - 1 : 0);
+    exb.t = __shfl_sync(0xFFFFFFFFu, wv.t, warp > 0 ? warp - 1 : 0);
     CState ex;
     bool has = false;
     if (warp > 0) {
-        ex = ws[warp];
+        ex = exb;
         has = true;
     }
     if (lane > 0) {
