@@ -191,9 +191,12 @@ cudaError_t launch_r3_inv(cudaStream_t s, u64* buf, int logm, const RootTables& 
 cudaError_t launch_mul_small(int logn, const PassGeo& g, cudaStream_t s, const u32* a, u64 na, const u32* b, u64 nb,
                              u32* out, u64 nout, unsigned long long* out_len, u64 ninv, const RootTables& tw,
                              const ProdJob* jobs = nullptr, unsigned njobs = 1);
+// The coefficients in `coef` are the unscaled inverse transform of `points`
+// points (N * c mod p); the carry scales them by points^-1 (points = 1: as
+// they are).
 cudaError_t launch_carry(unsigned nchunks, cudaStream_t s, const u64* coef, u32* out, u64 nout,
                          LookbackSlot* slots, u32* ticket, unsigned long long* out_len, u32* err,
-                         const ProdJob* jobs = nullptr, unsigned njobs = 1);
+                         const ProdJob* jobs = nullptr, unsigned njobs = 1, u64 points = 1);
 cudaError_t configure_first();
 cudaError_t configure_mid();
 cudaError_t configure_inv();

@@ -255,6 +255,18 @@ GL_FN u64 gl_shl(u64 x, int s) {
 #endif
 }
 
+// x * 2^(160 + t) for x < 2^64 and a run-time 0 <= t < 32, canonical, branch
+// free: 2^(160+t) = -2^(64+t), and gl_shl_w2's value A - B negated is B - A
+// (A = W0*2^32 <= p - 1 is a valid subtrahend, B < p). This is N^-1 = 2^(192-k)
+// for N = 2^k.
+__device__ __forceinline__ u64 gl_shl_160(u64 x, int t) {
+    const u32 x0 = (u32)x, x1 = (u32)(x >> 32);
+    const u32 W0 = x0 << t, W1 = __funnelshift_l(x0, x1, t), W2 = __funnelshift_l(x1, 0u, t);
+    u32 l, c;
+    asm("add.cc.u32 %0, %2, %3;\n\taddc.u32 %1, 0, 0;" : "=r"(l), "=r"(c) : "r"(W0), "r"(W1));
+    return gl_sub(((u64)(W2 + c) << 32) | l, (u64)W0 << 32);
+}
+
 // x * 2^s for x < 2^64 and a run-time, warp-uniform 0 <= s < 192: one copy
 // of the three word-offset folds behind uniform branches (t = 0 needs no
 // case of its own: the funnel shifts give W2 = 0 and the folds stay exact),

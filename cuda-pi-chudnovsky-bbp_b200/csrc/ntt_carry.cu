@@ -32,7 +32,7 @@ constexpr int LOOKBACK_SPIN_LIMIT = 1 << 22;
 __global__ void __launch_bounds__(CARRY_THREADS, 8) k_carry(const u64* __restrict__ coef, u32* __restrict__ out,
                                                          u64 nout, LookbackSlot* slots, u32* ticket,
                                                          unsigned long long* out_len, u32* err,
-                                                         const ProdJob* __restrict__ jobs) {
+                                                         const ProdJob* __restrict__ jobs, u64 ninv, int nshift) {
     if (jobs) {
         const ProdJob& J = jobs[blockIdx.y];
         coef = J.bufB;
@@ -57,6 +57,19 @@ __global__ void __launch_bounds__(CARRY_THREADS, 8) k_carry(const u64* __restric
         ulonglong2 p = src[i];
         cf[2 * i] = p.x;
         cf[2 * i + 1] = p.y;
+    }
+    // The inverse transform leaves N * c (mod p); the scale by N^-1 is done
+    // here rather than in the ALU-bound fused pass: for N = 2^k it is the
+    // shift by 2^(192 - k) (2 has order 192), otherwise one multiply.
+    if (nshift >= 160) {
+#pragma unroll
+        for (int i = 0; i < CARRY_G; ++i) cf[i] = gl_shl_160(cf[i], nshift - 160);
+    } else if (nshift > 0) {
+#pragma unroll
+        for (int i = 0; i < CARRY_G; ++i) cf[i] = gl_shl_rt(cf[i], (u32)nshift);
+    } else if (nshift < 0) {
+#pragma unroll
+        for (int i = 0; i < CARRY_G; ++i) cf[i] = gl_mul(cf[i], ninv);
     }
     u32 lm[CARRY_G / 2];
     const CState st = group_carry<CARRY_G>(cf, lm);
@@ -143,8 +156,22 @@ __global__ void __launch_bounds__(CARRY_THREADS, 8) k_carry(const u64* __restric
 
 cudaError_t launch_carry(unsigned nchunks, cudaStream_t s, const u64* coef, u32* out, u64 nout,
                          LookbackSlot* slots, u32* ticket, unsigned long long* out_len, u32* err,
-                         const ProdJob* jobs, unsigned njobs) {
-    k_carry<<<dim3(nchunks, njobs), CARRY_THREADS, 0, s>>>(coef, out, nout, slots, ticket, out_len, err, jobs);
+                         const ProdJob* jobs, unsigned njobs, u64 points) {
+    // scale by points^-1: a shift when points is a power of two
+    int nshift = 0;
+    u64 ninv = 1;
+    if (points > 1) {
+        if ((points & (points - 1)) == 0) {
+            int k = 0;
+            while ((1ull << k) < points) ++k;
+            nshift = 192 - k;
+        } else {
+            nshift = -1;
+            ninv = gl_inv(points);
+        }
+    }
+    k_carry<<<dim3(nchunks, njobs), CARRY_THREADS, 0, s>>>(coef, out, nout, slots, ticket, out_len, err, jobs, ninv,
+                                                           nshift);
     return cudaGetLastError();
 }
 

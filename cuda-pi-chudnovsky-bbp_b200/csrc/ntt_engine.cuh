@@ -31,13 +31,22 @@ namespace b2m {
 // Register DFTs on E = 2^e consecutive registers.
 // dft_fwd: natural-order input, bit-reversed output (decimation in frequency).
 // dft_inv: bit-reversed input, natural-order output (decimation in time),
-//          inverse roots, unscaled (1/N is folded into the pointwise step).
+//          inverse roots, unscaled (1/N is applied by the carry kernel, or by
+//          the pointwise step of the one-CTA product).
 // The root of unity of order 2h is 2^(96/h).
 // ---------------------------------------------------------------------------
-template <int E>
+// ZH: the upper half x[E/2 .. E) is known to be zero (the first level of the
+// first forward pass, whose input holds at most N/2 digits): the first level
+// is then x[j + E/2] = x[j] * w^j, no additions.
+template <int E, bool ZH = false>
 GL_FN void dft_fwd(u64* x) {
+    if constexpr (ZH) {
 #pragma unroll
-    for (int h = E / 2; h >= 1; h >>= 1) {
+        for (int j = 1; j < E / 2; ++j) x[j + E / 2] = gl_shl(x[j], (96 * j) / (E / 2));
+        x[E / 2] = x[0];
+    }
+#pragma unroll
+    for (int h = ZH ? E / 4 : E / 2; h >= 1; h >>= 1) {
 #pragma unroll
         for (int b = 0; b < E; b += 2 * h) {
 #pragma unroll
@@ -153,7 +162,7 @@ struct Steps {
 // j in [0, R/2^A); elements at rows j + m*(R/2^A). Forward: DFT then
 // w_R^(j*k); inverse: w_R^(-j*k) then inverse DFT.
 // ---------------------------------------------------------------------------
-template <class TL, int A, bool INV>
+template <class TL, int A, bool INV, bool ZH = false>
 __device__ __forceinline__ void lead_step(u64* sm, const u64* __restrict__ dtw) {
     constexpr int E = 1 << A, R = TL::R, LOGJ = TL::LR - A, JW = R >> A;
     for_tasks<(JW << TL::LC), TL::T>([&](int q) {
@@ -169,9 +178,9 @@ __device__ __forceinline__ void lead_step(u64* sm, const u64* __restrict__ dtw) 
         u64* ptr = sm + TL::saddr(j, col);
         constexpr int st = TL::template step<JW>();
 #pragma unroll
-        for (int m = 0; m < E; ++m) x[m] = ptr[m * st];
+        for (int m = 0; m < (ZH ? E / 2 : E); ++m) x[m] = ptr[m * st];
         if (!INV) {
-            dft_fwd<E>(x);
+            dft_fwd<E, ZH>(x);
 #pragma unroll
             for (int i = 1; i < E; ++i) x[i] = gl_mul(x[i], __ldg(dtw + R + ((j * brev_c(i, A)) & (R - 1))));
         } else {
@@ -239,7 +248,7 @@ __device__ __forceinline__ void level1_twiddle(u64* x, int u1) {
 // Task order puts the level index (u1 or i1) outermost so it is uniform
 // across a warp whenever the tile has >= 32 instances.
 // ---------------------------------------------------------------------------
-template <class TL, int LOGL, bool INV, bool RT>
+template <class TL, int LOGL, bool INV, bool RT, bool ZH = false>
 __device__ __forceinline__ void group64(u64* sm, const u64* __restrict__ dtw) {
     constexpr int L = 1 << LOGL, LOGJ = LOGL - 6, JW = 1 << LOGJ;
     constexpr int LOGNI = TL::LR - 6 + TL::LC;  // instances = C * R / 64
@@ -254,9 +263,9 @@ __device__ __forceinline__ void group64(u64* sm, const u64* __restrict__ dtw) {
             constexpr int st = TL::template step<8 * JW>();
             u64 x[8];
 #pragma unroll
-            for (int m = 0; m < 8; ++m) x[m] = ptr[m * st];
+            for (int m = 0; m < (ZH ? 4 : 8); ++m) x[m] = ptr[m * st];
             if (!INV) {
-                dft_fwd<8>(x);
+                dft_fwd<8, ZH>(x);
                 level1_twiddle<false, RT>(x, u1);
             } else {
                 level1_twiddle<true, RT>(x, u1);
@@ -337,10 +346,10 @@ __device__ __forceinline__ void lone8(u64* sm) {
 }
 
 // Radix-64 groups from block size 2^LOGL down, G groups.
-template <class TL, int LOGL, int G, bool RT>
+template <class TL, int LOGL, int G, bool RT, bool ZH = false>
 __device__ __forceinline__ void groups_fwd(u64* sm, const u64* dtw) {
     if constexpr (G > 0) {
-        group64<TL, LOGL, false, RT>(sm, dtw);
+        group64<TL, LOGL, false, RT, ZH>(sm, dtw);
         __syncthreads();
         groups_fwd<TL, LOGL - 6, G - 1, RT>(sm, dtw);
     }
@@ -361,14 +370,20 @@ __device__ __forceinline__ void groups_inv(u64* sm, const u64* dtw) {
 // radix-64 group keep the specialised bodies, tiles with two groups (whose
 // specialised code stalled on instruction fetch) and all inverse tiles use
 // the run-time shifts.
-template <class TL, bool RT = (Steps<TL::LR>::G >= 2)>
+// ZH: rows [R/2, R) of every column are zero (first forward pass of an
+// operand holding at most N/2 digits), so the first butterfly level of the
+// column DFT -- in the lead step, or in the first group when there is none --
+// has no additions and its zero half is not read.
+template <class TL, bool RT = (Steps<TL::LR>::G >= 2), bool ZH = false>
 __device__ __forceinline__ void tile_fwd(u64* sm, const u64* dtw) {
     using S = Steps<TL::LR>;
     if constexpr (S::A > 0) {
-        lead_step<TL, S::A, false>(sm, dtw);
+        lead_step<TL, S::A, false, ZH>(sm, dtw);
         __syncthreads();
+        groups_fwd<TL, TL::LR - S::A, S::G, RT>(sm, dtw);
+    } else {
+        groups_fwd<TL, TL::LR - S::A, S::G, RT, ZH>(sm, dtw);
     }
-    groups_fwd<TL, TL::LR - S::A, S::G, RT>(sm, dtw);
     if constexpr (S::LONE) {
         lone8<TL, false>(sm);
         __syncthreads();

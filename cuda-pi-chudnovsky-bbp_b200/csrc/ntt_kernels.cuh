@@ -5,10 +5,10 @@
 //   A: k_fwd_first (u32 limbs -> 16-bit digits -> pass 1), k_fwd_mid ...,
 //      k_fwd_last (last pass)
 //   B: k_fwd_first, k_fwd_mid ..., k_fused_last (last forward pass, pointwise
-//      product with A's spectrum and 1/N, first inverse pass, in one tile)
-//   inverse: k_inv_mid for the remaining passes (pass 1 yields the
-//      coefficients in natural order), k_carry (decoupled-lookback carry into
-//      u32 limbs + trimmed length).
+//      product with A's spectrum, first inverse pass, in one tile)
+//   inverse: k_inv_mid for the remaining passes (pass 1 yields N times the
+//      coefficients in natural order), k_carry (scale by 1/N, then the
+//      decoupled-lookback carry into u32 limbs + trimmed length).
 // For N <= 2^13 one CTA does the whole product (k_mul_small).
 //
 // Every pass kernel: a cooperative, coalesced load of its R x C tile into
@@ -127,7 +127,10 @@ k_fwd_first(const u32* __restrict__ limbs, u64 ndig, u64* __restrict__ out, int 
 #pragma unroll
     for (int k = 0; k < G::PER; ++k) sm[gp.sa0 + G::soff(k)] = digit_of(limbs, ndig, gp.gi0 + k * gp.gstep);
     __syncthreads();
-    tile_fwd<TL>(sm, tw.dtw);
+    // The digits fill at most half of the transform for almost every product
+    // (N >= 2 (na + nb)): rows [R/2, R) of every column are then zero.
+    if (2 * ndig <= (1ull << logM)) tile_fwd<TL, (Steps<LOGR>::G >= 2), true>(sm, tw.dtw);
+    else tile_fwd<TL>(sm, tw.dtw);
     if (ttab) {
 #pragma unroll
         for (int k = 0; k < G::PER; ++k)
@@ -175,8 +178,8 @@ k_fwd_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const u64* _
 }
 
 // A not-last inverse pass, in place: inverse inter-pass twiddle on load, then
-// the inverse column DFTs. Pass 1 of the inverse leaves the convolution
-// coefficients (N^-1 already applied) in natural order.
+// the inverse column DFTs. Pass 1 of the inverse leaves N times the
+// convolution coefficients (mod p) in natural order; the carry kernel scales.
 template <int LOGR, int LOGC>
 __global__ void B2M_PASS_BOUNDS((Tile<LOGR, LOGC, MAP_COL>::T))
 k_inv_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const u64* __restrict__ ttab,
@@ -238,7 +241,8 @@ k_fwd_last(u64* __restrict__ buf, RootTables tw, const ProdJob* __restrict__ job
 }
 
 // Last forward pass of operand B, pointwise product with A's spectrum (same
-// positions) and N^-1, then the first inverse pass -- one tile, one kernel.
+// positions; times ninv unless ninv is 1, i.e. unless the carry kernel applies
+// N^-1), then the first inverse pass -- one tile, one kernel.
 // aspec null (no job table): a square, B's spectrum times itself.
 template <int LOGR, int LOGC>
 __global__ void B2M_PASS_BOUNDS((Tile<LOGR, LOGC, MAP_ROW>::T))
@@ -263,17 +267,20 @@ k_fused_last(u64* __restrict__ bbuf, const u64* __restrict__ aspec, u64 ninv, Ro
     cp_async_wait_all();
     __syncthreads();
     tile_fwd<TL, true>(sm, tw.dtw);
+    // ninv == 1: the carry kernel applies N^-1 (single products and batches)
     if (square) {
 #pragma unroll
         for (int k = 0; k < G::PER; ++k) {
             u64& v = sm[gp.sa0 + G::soff(k)];
-            v = gl_mul(gl_mul(v, v), ninv);
+            v = gl_mul(v, v);
+            if (ninv != 1) v = gl_mul(v, ninv);
         }
     } else {
 #pragma unroll
         for (int k = 0; k < G::PER; ++k) {
             u64& v = sm[gp.sa0 + G::soff(k)];
-            v = gl_mul(gl_mul(v, __ldg(abase + k * TL::T)), ninv);
+            v = gl_mul(v, __ldg(abase + k * TL::T));
+            if (ninv != 1) v = gl_mul(v, ninv);
         }
     }
     __syncthreads();

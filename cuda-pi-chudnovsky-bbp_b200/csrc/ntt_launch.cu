@@ -342,11 +342,11 @@ cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb,
     if (a == b && na == nb) {
         // a square: one forward transform, its spectrum squared in the fused pass
         if (b_ready && (e = cudaStreamWaitEvent(s, b_ready, 0)) != cudaSuccess) return e;
-        if ((e = launch_forward(b, nb, bufB, p, tw, true, nullptr, ninv, s, tr)) != cudaSuccess) return e;
+        if ((e = launch_forward(b, nb, bufB, p, tw, true, nullptr, 1, s, tr)) != cudaSuccess) return e;
     } else {
         if ((e = launch_forward(a, na, bufA, p, tw, false, nullptr, 0, s, tr)) != cudaSuccess) return e;
         if (b_ready && (e = cudaStreamWaitEvent(s, b_ready, 0)) != cudaSuccess) return e;
-        if ((e = launch_forward(b, nb, bufB, p, tw, true, bufA, ninv, s, tr)) != cudaSuccess) return e;
+        if ((e = launch_forward(b, nb, bufB, p, tw, true, bufA, 1, s, tr)) != cudaSuccess) return e;
     }
     for (int k = p.npass - 2; k >= 0; --k) {
         if (tr) tr->mark(s, B2M_K_INV_MID, p.logr[k]);
@@ -357,7 +357,7 @@ cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb,
         if ((e = launch_r3_inv(s, bufB, logn, tw)) != cudaSuccess) return e;
     }
     if (tr) tr->mark(s, B2M_K_CARRY, 0);
-    e = launch_carry((unsigned)nchunks, s, bufB, out, nout, slots, ticket, ol, err);
+    e = launch_carry((unsigned)nchunks, s, bufB, out, nout, slots, ticket, ol, err, nullptr, 1, n);
     if (tr) tr->end(s);
     return e;
 }
@@ -404,13 +404,13 @@ cudaError_t launch_bucket(const Plan& p, const ProdJob* jobs, unsigned njobs, co
     }
     cudaError_t e = cudaSuccess;
     for (int op = a_ready ? 1 : 0; op < 2 && e == cudaSuccess; ++op)
-        e = bucket_forward(p, jobs, njobs, tw, s, op, ninv);
+        e = bucket_forward(p, jobs, njobs, tw, s, op, 1);  // N^-1: in the carry
     for (int k = p.npass - 2; e == cudaSuccess && k >= 0; --k)
         e = launch_inv_mid(p.logr[k], geo(p, k), s, nullptr, tw, jobs, njobs);
     if (e == cudaSuccess && p.three) e = launch_r3_inv(s, nullptr, logn, tw, jobs, njobs);
     if (e != cudaSuccess) return e;
     const unsigned nchunks = (unsigned)(plan_points(p) / CARRY_CHUNK);
-    return launch_carry(nchunks, s, nullptr, nullptr, 0, nullptr, nullptr, nullptr, err, jobs, njobs);
+    return launch_carry(nchunks, s, nullptr, nullptr, 0, nullptr, nullptr, nullptr, err, jobs, njobs, plan_points(p));
 }
 
 // Zero a contiguous carry-scratch region and every job's out_len

@@ -67,6 +67,9 @@ def test_every_shift_amount(b2m_gpu):
     assert ints(b2m_gpu.field_eval("shl", arr(xs), arr(ss))) == want
     # the run-time (warp-uniform) shift of the level-1 twiddles
     assert ints(b2m_gpu.field_eval("shl_rt", arr(xs), arr(ss))) == want
+    # the carry's scale by N^-1 = 2^(192 - k): x * 2^(160 + t), t < 32
+    ts = [s % 32 for s in ss]
+    assert ints(b2m_gpu.field_eval("shl_160", arr(xs), arr(ts))) == [(x << (160 + t)) % P for x, t in zip(xs, ts)]
 
 
 def test_random_pairs(b2m_gpu):
