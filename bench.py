@@ -364,8 +364,7 @@ def run_ours(args) -> None:
             "data": "synthetic: seeded uniform random u32 limbs (splitmix64), top limb non-zero",
             "config": {"workload": workload, "na": na, "nb": nb,
                        "ntt_length": n, "plan": plan, "products_per_step": world,
-                       "autotune": ({"candidates": len(tune), "best_ms": min(t["ms"] for t in tune),
-                                     "worst_ms": max(t["ms"] for t in tune)} if tune else None),
+                       "autotune": (autotune_summary(tune) if tune else None),
                        "glimbs_per_s": round((na + nb) * world / (step_ms * 1e-3) / 1e9, 3),
                        "l2": f"working set {wset / 2**20:.0f} MiB per product "
                              + ("> 126 MB L2: no flush needed" if wset > 126 * 2**20
@@ -391,6 +390,19 @@ def run_ours(args) -> None:
         }
         print(json.dumps(line), flush=True)
     ranks.close(rk)
+
+
+def autotune_summary(tune: list) -> dict:
+    """Best and worst candidate, and the best of each pass count."""
+    def best(c):
+        t = min(c, key=lambda t: t["ms"])
+        return {"logr": t["logr"], "logc": t["logc"], "ms": t["ms"]}
+    out = {"candidates": len(tune), "best_ms": min(t["ms"] for t in tune), "worst_ms": max(t["ms"] for t in tune)}
+    for k in (2, 3):
+        c = [t for t in tune if len(t["logr"]) == k]
+        if c:
+            out[f"best_{k}_pass"] = best(c)
+    return out
 
 
 def batch_sizes(n: int, seed: int):

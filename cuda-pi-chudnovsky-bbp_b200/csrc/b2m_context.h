@@ -32,6 +32,11 @@ struct Context {
         u64* fwd;
         u64* inv;
         uint64_t bytes;
+        // inv times 2^-logm, for the table's use as pass 0 of a 2^logm-point
+        // transform (the inverse pass 0 then applies N^-1 for free); built by
+        // twtable_ensure for pass 0, null until then or if the budget is short
+        u64* inv0 = nullptr;
+        uint64_t inv0_bytes = 0;
     };
     std::mutex twt_mu;
     std::vector<TwTable> twt;

@@ -152,6 +152,10 @@ struct PassGeo {
     // (logm, logr); null: the kernels build each twiddle from u1 * u2.
     const u64* tfwd = nullptr;
     const u64* tinv = nullptr;
+    // Pass 0 only: the inverse table times 2^-logm (see Context::TwTable),
+    // when it exists; an inverse pass 0 run with it leaves the coefficients
+    // already scaled by the sub-transform's 2^-logn.
+    const u64* tinv0 = nullptr;
     // Radix-3 plans: grid z runs over the three sub-transforms, zstride
     // elements apart (1 and 0 otherwise).
     unsigned zdim = 1;

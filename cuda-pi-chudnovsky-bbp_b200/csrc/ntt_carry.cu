@@ -29,6 +29,12 @@ __device__ __forceinline__ void st_release(u32* p, u32 v) {
 
 constexpr int LOOKBACK_SPIN_LIMIT = 1 << 22;
 
+// SC: how the coefficients are scaled by N^-1 before the carry -- 0 not at all
+// (the last inverse pass already did, through its scaled twiddle table),
+// 1 by 2^nshift with nshift >= 160 (N a power of two), 2 by the multiply with
+// ninv. A template parameter, so that the common unscaled kernel keeps all of
+// its 32 registers (eight CTAs per SM) for the carry itself.
+template <int SC>
 __global__ void __launch_bounds__(CARRY_THREADS, 8) k_carry(const u64* __restrict__ coef, u32* __restrict__ out,
                                                          u64 nout, LookbackSlot* slots, u32* ticket,
                                                          unsigned long long* out_len, u32* err,
@@ -61,13 +67,10 @@ __global__ void __launch_bounds__(CARRY_THREADS, 8) k_carry(const u64* __restric
     // The inverse transform leaves N * c (mod p); the scale by N^-1 is done
     // here rather than in the ALU-bound fused pass: for N = 2^k it is the
     // shift by 2^(192 - k) (2 has order 192), otherwise one multiply.
-    if (nshift >= 160) {
+    if constexpr (SC == 1) {
 #pragma unroll
         for (int i = 0; i < CARRY_G; ++i) cf[i] = gl_shl_160(cf[i], nshift - 160);
-    } else if (nshift > 0) {
-#pragma unroll
-        for (int i = 0; i < CARRY_G; ++i) cf[i] = gl_shl_rt(cf[i], (u32)nshift);
-    } else if (nshift < 0) {
+    } else if constexpr (SC == 2) {
 #pragma unroll
         for (int i = 0; i < CARRY_G; ++i) cf[i] = gl_mul(cf[i], ninv);
     }
@@ -157,21 +160,19 @@ __global__ void __launch_bounds__(CARRY_THREADS, 8) k_carry(const u64* __restric
 cudaError_t launch_carry(unsigned nchunks, cudaStream_t s, const u64* coef, u32* out, u64 nout,
                          LookbackSlot* slots, u32* ticket, unsigned long long* out_len, u32* err,
                          const ProdJob* jobs, unsigned njobs, u64 points) {
-    // scale by points^-1: a shift when points is a power of two
-    int nshift = 0;
-    u64 ninv = 1;
-    if (points > 1) {
-        if ((points & (points - 1)) == 0) {
-            int k = 0;
-            while ((1ull << k) < points) ++k;
-            nshift = 192 - k;
-        } else {
-            nshift = -1;
-            ninv = gl_inv(points);
-        }
+    // scale by points^-1: a shift when points is a power of two (2^(192 - k),
+    // k <= 32, is a shift by 160 + (32 - k)), else one multiply
+    const dim3 grid(nchunks, njobs);
+    if (points <= 1) {
+        k_carry<0><<<grid, CARRY_THREADS, 0, s>>>(coef, out, nout, slots, ticket, out_len, err, jobs, 1, 0);
+    } else if ((points & (points - 1)) == 0 && points <= (1ull << 32)) {
+        int k = 0;
+        while ((1ull << k) < points) ++k;
+        k_carry<1><<<grid, CARRY_THREADS, 0, s>>>(coef, out, nout, slots, ticket, out_len, err, jobs, 1, 192 - k);
+    } else {
+        k_carry<2><<<grid, CARRY_THREADS, 0, s>>>(coef, out, nout, slots, ticket, out_len, err, jobs, gl_inv(points),
+                                                  -1);
     }
-    k_carry<<<dim3(nchunks, njobs), CARRY_THREADS, 0, s>>>(coef, out, nout, slots, ticket, out_len, err, jobs, ninv,
-                                                           nshift);
     return cudaGetLastError();
 }
 

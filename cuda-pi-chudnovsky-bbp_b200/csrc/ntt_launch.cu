@@ -163,6 +163,7 @@ PassGeo pass_geo(const Plan& p, int k) {
             if (t.logm == g.logm && t.logr == g.logr) {
                 g.tfwd = t.fwd;
                 g.tinv = t.inv;
+                if (k == 0) g.tinv0 = t.inv0;
                 break;
             }
     }
@@ -181,6 +182,37 @@ __global__ void k_build_twtable(u64* __restrict__ fwd, u64* __restrict__ inv, in
         fwd[i] = e ? uroot(e, tw.u1, tw.u2) : 1ull;
         inv[i] = e ? uroot(0u - e, tw.u1, tw.u2) : 1ull;
     }
+}
+
+__global__ void k_scale_table(u64* __restrict__ dst, const u64* __restrict__ src, u64 m, int shift) {
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (u64)gridDim.x * blockDim.x)
+        dst[i] = gl_shl(src[i], shift);
+}
+
+// The pass-0 copy of an existing inverse table, scaled by 2^-logm (= 2^(192 -
+// logm), a shift); skipped when the budget is short.
+static cudaError_t twtable_ensure_inv0(Context* c, Context::TwTable& t, cudaStream_t s) {
+    if (t.inv0) return cudaSuccess;
+    const uint64_t bytes = 8ull << t.logm;
+    if (!budget_reserve(c, bytes)) return cudaSuccess;
+    u64* mem = nullptr;
+    cudaError_t e = cudaMalloc(&mem, bytes);
+    if (e != cudaSuccess) {
+        budget_release(c, bytes);
+        cudaGetLastError();
+        return cudaSuccess;
+    }
+    const u64 m = 1ull << t.logm;
+    k_scale_table<<<(unsigned)std::min<u64>(65535, (m + 255) / 256), 256, 0, s>>>(mem, t.inv, m, 192 - t.logm);
+    if ((e = cudaGetLastError()) == cudaSuccess) e = cudaStreamSynchronize(s);  // built before anyone sees it
+    if (e != cudaSuccess) {
+        cudaFree(mem);
+        budget_release(c, bytes);
+        return e;
+    }
+    t.inv0 = mem;
+    t.inv0_bytes = bytes;
+    return cudaSuccess;
 }
 
 cudaError_t twtable_ensure(Context* c, const Plan& p, cudaStream_t s) {
@@ -214,6 +246,19 @@ cudaError_t twtable_ensure(Context* c, const Plan& p, cudaStream_t s) {
         }
         c->twt.push_back({g.logm, g.logr, mem, mem + m, bytes});
     }
+    // the scaled inverse copy for pass 0
+    if (p.npass >= 2) {
+        const PassGeo g = pass_geo(p, 0);
+        if (g.tinv && !g.tinv0) {
+            std::lock_guard<std::mutex> lk(c->twt_mu);
+            for (Context::TwTable& t : c->twt)
+                if (t.logm == g.logm && t.logr == g.logr) {
+                    cudaError_t e = twtable_ensure_inv0(c, t, s);
+                    if (e != cudaSuccess) return e;
+                    break;
+                }
+        }
+    }
     return cudaSuccess;
 }
 
@@ -222,6 +267,10 @@ void twtable_free_all(Context* c) {
     for (const Context::TwTable& t : c->twt) {
         cudaFree(t.fwd);
         budget_release(c, t.bytes);
+        if (t.inv0) {
+            cudaFree(t.inv0);
+            budget_release(c, t.inv0_bytes);
+        }
     }
     c->twt.clear();
 }
@@ -257,6 +306,20 @@ static PassGeo geo(const Plan& p, int k) {
     if (p.three) {
         g.zdim = 3;
         g.zstride = 1ull << p.logn;
+    }
+    return g;
+}
+
+// Geometry of inverse pass k. For pass 0 with a scaled inverse table
+// (PassGeo::tinv0) the pass applies 2^-logn with its twiddles, and
+// *carry_scale, the factor the carry kernel divides by, drops to what is
+// left (3 for a 3 * 2^logn transform, else 1). The table is looked up once
+// here, so the pass and the carry agree.
+static PassGeo inverse_geo(const Plan& p, int k, uint64_t* carry_scale) {
+    PassGeo g = geo(p, k);
+    if (k == 0 && g.tinv0) {
+        g.tinv = g.tinv0;
+        *carry_scale = p.three ? 3 : 1;
     }
     return g;
 }
@@ -348,16 +411,17 @@ cudaError_t launch_product(const u32* a, uint64_t na, const u32* b, uint64_t nb,
         if (b_ready && (e = cudaStreamWaitEvent(s, b_ready, 0)) != cudaSuccess) return e;
         if ((e = launch_forward(b, nb, bufB, p, tw, true, bufA, 1, s, tr)) != cudaSuccess) return e;
     }
+    uint64_t carry_scale = n;  // the factor the carry still divides by
     for (int k = p.npass - 2; k >= 0; --k) {
         if (tr) tr->mark(s, B2M_K_INV_MID, p.logr[k]);
-        if ((e = launch_inv_mid(p.logr[k], geo(p, k), s, bufB, tw)) != cudaSuccess) return e;
+        if ((e = launch_inv_mid(p.logr[k], inverse_geo(p, k, &carry_scale), s, bufB, tw)) != cudaSuccess) return e;
     }
     if (p.three) {
         if (tr) tr->mark(s, B2M_K_R3_INV, 0);
         if ((e = launch_r3_inv(s, bufB, logn, tw)) != cudaSuccess) return e;
     }
     if (tr) tr->mark(s, B2M_K_CARRY, 0);
-    e = launch_carry((unsigned)nchunks, s, bufB, out, nout, slots, ticket, ol, err, nullptr, 1, n);
+    e = launch_carry((unsigned)nchunks, s, bufB, out, nout, slots, ticket, ol, err, nullptr, 1, carry_scale);
     if (tr) tr->end(s);
     return e;
 }
@@ -405,12 +469,13 @@ cudaError_t launch_bucket(const Plan& p, const ProdJob* jobs, unsigned njobs, co
     cudaError_t e = cudaSuccess;
     for (int op = a_ready ? 1 : 0; op < 2 && e == cudaSuccess; ++op)
         e = bucket_forward(p, jobs, njobs, tw, s, op, 1);  // N^-1: in the carry
+    uint64_t carry_scale = plan_points(p);
     for (int k = p.npass - 2; e == cudaSuccess && k >= 0; --k)
-        e = launch_inv_mid(p.logr[k], geo(p, k), s, nullptr, tw, jobs, njobs);
+        e = launch_inv_mid(p.logr[k], inverse_geo(p, k, &carry_scale), s, nullptr, tw, jobs, njobs);
     if (e == cudaSuccess && p.three) e = launch_r3_inv(s, nullptr, logn, tw, jobs, njobs);
     if (e != cudaSuccess) return e;
     const unsigned nchunks = (unsigned)(plan_points(p) / CARRY_CHUNK);
-    return launch_carry(nchunks, s, nullptr, nullptr, 0, nullptr, nullptr, nullptr, err, jobs, njobs, plan_points(p));
+    return launch_carry(nchunks, s, nullptr, nullptr, 0, nullptr, nullptr, nullptr, err, jobs, njobs, carry_scale);
 }
 
 // Zero a contiguous carry-scratch region and every job's out_len
