@@ -298,8 +298,8 @@ b2m_status b2m_selftest_wait_timeout(b2m_stream stream) {
     cudaSetDevice(c->device);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     // Two chunks of (zero) coefficients and their lookback slots, the ticket
-    // starting at 1: the one CTA launched takes chunk 1 and waits for chunk
-    // 0's flag, which nothing ever sets.
+    // starting at 1: the CTA that takes chunk 1 waits for chunk 0's flag,
+    // which nothing ever sets (no CTA is left to take ticket 0).
     const uint64_t n = 2 * (uint64_t)CARRY_CHUNK;
     auto al = [](uint64_t x) { return (x + 255) & ~255ull; };
     const uint64_t bc = al(8 * n), bo = al(4 * (n / 2)), bs = al(2 * sizeof(LookbackSlot)), bt = 256;
@@ -312,7 +312,7 @@ b2m_status b2m_selftest_wait_timeout(b2m_stream stream) {
     e = cudaMemsetAsync(mem, 0, bc + bo + bs + bt, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(ticket, &one, 4, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
-        e = launch_carry(1, s, reinterpret_cast<const u64*>(b), reinterpret_cast<u32*>(b + bc), n / 2,
+        e = launch_carry(2, s, reinterpret_cast<const u64*>(b), reinterpret_cast<u32*>(b + bc), n / 2,
                          reinterpret_cast<LookbackSlot*>(b + bc + bo), ticket,
                          reinterpret_cast<unsigned long long*>(ticket + 2), c->d_err);
     cudaFreeAsync(mem, s);

@@ -12,33 +12,119 @@ namespace b2m {
 
 // ---------------------------------------------------------------------------
 // Carry: coefficients (natural order, N of them) -> nout u32 limbs.
-// One CTA per 4096 coefficients, chunks claimed in launch order by ticket so
-// that every chunk a CTA waits for belongs to a CTA that is already running
-// and publishes its aggregate without waiting. Waits are bounded: after
-// ~2^22 polls the kernel flags *err and carries on with a wrong carry (the
-// host turns the flag into B2M_ERR_DEVICE_TIMEOUT).
+// One CTA per chunk of 4096 coefficients, chunks claimed in launch order by
+// ticket so that every chunk a CTA waits for belongs to a CTA that is already
+// running and publishes its aggregate without waiting. Waits are bounded:
+// after ~2^22 polls the kernel flags *err and carries on with a wrong carry
+// (the host turns the flag into B2M_ERR_DEVICE_TIMEOUT).
+//
+// Each thread normalises 16 contiguous coefficients, but the chunk is read
+// coalesced (lane l of a warp reads pair i*32 + l of the warp's 512
+// coefficients) and handed to its owner through shared memory: a thread's
+// own 128 contiguous bytes read directly would touch 32 cache lines per warp
+// load instruction, eight times the L1 wavefronts of the coalesced read.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ u32 ld_acquire(const u32* p) {
     u32 v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+// Release store: the thread's earlier writes (the slot's values) are visible
+// to any thread that reads this flag with ld_acquire.
 __device__ __forceinline__ void st_release(u32* p, u32 v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 constexpr int LOOKBACK_SPIN_LIMIT = 1 << 22;
+constexpr int CARRY_WARP_PAIRS = 32 * CARRY_G / 2;  // coefficient pairs per warp
+constexpr int CARRY_MIN_CTAS = CARRY_G >= 16 ? 6 : 8;  // CTAs per SM the staging area allows
+
+// The warp's 32 * CARRY_G coefficients from HBM into cf[] of their owner
+// lane (lane l owns coefficients CARRY_G*l .. CARRY_G*l + CARRY_G - 1 of the
+// warp's slice). Pair q of the slice belongs to lane o = q / PPL as its pair
+// j = q % PPL (PPL = CARRY_G / 2 pairs per lane) and sits in slot
+// o*PPL + (j ^ ((o / (8/PPL)) % PPL)) of the warp's staging area: both the
+// coalesced stores and the owners' reads touch eight distinct 16-byte bank
+// groups per quarter warp.
+__device__ __forceinline__ void load_chunk(const u64* __restrict__ coef, u64 wbase, ulonglong2* stage, u64* cf) {
+    constexpr int PPL = CARRY_G / 2, OPR = 8 / PPL;  // pairs per lane, owners per 128-byte row
+    static_assert(PPL == 4 || PPL == 8, "staging layout for 8 or 16 coefficients per thread");
+    const int lane = threadIdx.x & 31;
+    const ulonglong2* src = reinterpret_cast<const ulonglong2*>(coef + wbase);
+    ulonglong2 v[PPL];
+#pragma unroll
+    for (int i = 0; i < PPL; ++i) v[i] = src[i * 32 + lane];
+#pragma unroll
+    for (int i = 0; i < PPL; ++i) {
+        const int o = i * (32 / PPL) + lane / PPL, j = lane % PPL;  // owner and pair of q = 32i + lane
+        stage[o * PPL + (j ^ ((o / OPR) % PPL))] = v[i];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < PPL; ++j) {
+        const ulonglong2 p = stage[lane * PPL + (j ^ ((lane / OPR) % PPL))];
+        cf[2 * j] = p.x;
+        cf[2 * j + 1] = p.y;
+    }
+}
+
+// Thread 0: publish chunk `chunk`'s aggregate, then walk back composing
+// predecessors' aggregates until an inclusive value or a carry-independent
+// (constant) composition is found; publish the inclusive value and return
+// the chunk's carry-in.
+__device__ __forceinline__ u64 chunk_lookback(LookbackSlot* slots, u32 chunk, CState agg, u32* err) {
+    if (chunk == 0) {
+        slots[0].incl = cs_eval(agg, 0);
+        st_release(&slots[0].flag, 2u);
+        return 0;
+    }
+    slots[chunk].agg_h = agg.h;
+    slots[chunk].agg_t = agg.t;
+    st_release(&slots[chunk].flag, 1u);
+    u64 cin = 0;
+    CState acc{0, CS_NEVER};
+    bool acc_id = true;
+    long p = (long)chunk - 1;
+    while (true) {
+        u32 f;
+        int spins = 0;
+        while ((f = ld_acquire(&slots[p].flag)) == 0u) {
+            if (++spins > LOOKBACK_SPIN_LIMIT) break;
+            __nanosleep(64);
+        }
+        if (f == 0u) {  // gave up: report, use 0 and finish cleanly
+            atomicOr(err, 1u);
+            cin = 0;
+            break;
+        }
+        if (f == 2u) {
+            const u64 val = *(volatile u64*)&slots[p].incl;
+            cin = acc_id ? val : cs_eval(acc, val);
+            break;
+        }
+        const CState a{*(volatile u64*)&slots[p].agg_h, *(volatile u64*)&slots[p].agg_t};
+        acc = acc_id ? a : cs_then(a, acc);
+        acc_id = false;
+        if (acc.t == CS_NEVER) {  // constant: earlier chunks cannot matter
+            cin = acc.h;
+            break;
+        }
+        --p;  // p > 0 here: chunk 0 always publishes inclusive
+    }
+    slots[chunk].incl = cs_eval(agg, cin);
+    st_release(&slots[chunk].flag, 2u);
+    return cin;
+}
 
 // SC: how the coefficients are scaled by N^-1 before the carry -- 0 not at all
 // (the last inverse pass already did, through its scaled twiddle table),
 // 1 by 2^nshift with nshift >= 160 (N a power of two), 2 by the multiply with
-// ninv. A template parameter, so that the common unscaled kernel keeps all of
-// its 32 registers (eight CTAs per SM) for the carry itself.
+// ninv.
 template <int SC>
-__global__ void __launch_bounds__(CARRY_THREADS, 8) k_carry(const u64* __restrict__ coef, u32* __restrict__ out,
-                                                         u64 nout, LookbackSlot* slots, u32* ticket,
-                                                         unsigned long long* out_len, u32* err,
-                                                         const ProdJob* __restrict__ jobs, u64 ninv, int nshift) {
+__global__ void __launch_bounds__(CARRY_THREADS, CARRY_MIN_CTAS)
+    k_carry(const u64* __restrict__ coef, u32* __restrict__ out, u64 nout, u32 nchunks, LookbackSlot* slots,
+            u32* ticket, unsigned long long* out_len, u32* err, const ProdJob* __restrict__ jobs, u64 ninv,
+            int nshift) {
     if (jobs) {
         const ProdJob& J = jobs[blockIdx.y];
         coef = J.bufB;
@@ -48,25 +134,22 @@ __global__ void __launch_bounds__(CARRY_THREADS, 8) k_carry(const u64* __restric
         ticket = J.ticket;
         out_len = J.out_len;
     }
+    __shared__ ulonglong2 s_stage[CARRY_THREADS / 32][CARRY_WARP_PAIRS];
     __shared__ u32 s_chunk;
     __shared__ u64 s_cin;
+    __shared__ unsigned long long s_top[CARRY_THREADS / 32];
     __shared__ CState s_ws[CARRY_THREADS / 32 + 1];
     if (threadIdx.x == 0) s_chunk = atomicAdd(ticket, 1u);
     __syncthreads();
     const u32 chunk = s_chunk;
+    if (chunk >= nchunks) return;
+    const int warp = threadIdx.x >> 5;
 
     u64 cf[CARRY_G];
-    const u64 cbase = (u64)chunk * CARRY_CHUNK + (u64)threadIdx.x * CARRY_G;
-    const ulonglong2* src = reinterpret_cast<const ulonglong2*>(coef + cbase);
-#pragma unroll
-    for (int i = 0; i < CARRY_G / 2; ++i) {
-        ulonglong2 p = src[i];
-        cf[2 * i] = p.x;
-        cf[2 * i + 1] = p.y;
-    }
-    // The inverse transform leaves N * c (mod p); the scale by N^-1 is done
-    // here rather than in the ALU-bound fused pass: for N = 2^k it is the
-    // shift by 2^(192 - k) (2 has order 192), otherwise one multiply.
+    load_chunk(coef, (u64)chunk * CARRY_CHUNK + (u64)warp * (32 * CARRY_G), s_stage[warp], cf);
+    // The inverse transform leaves N * c (mod p) unless its last pass
+    // already scaled: for N = 2^k the scale is the shift by 2^(192 - k)
+    // (2 has order 192), otherwise one multiply.
     if constexpr (SC == 1) {
 #pragma unroll
         for (int i = 0; i < CARRY_G; ++i) cf[i] = gl_shl_160(cf[i], nshift - 160);
@@ -79,61 +162,13 @@ __global__ void __launch_bounds__(CARRY_THREADS, 8) k_carry(const u64* __restric
     bool has_ex;
     CState agg;
     const CState ex = block_scan_carry(st, &has_ex, &agg, s_ws);
-
-    if (threadIdx.x == 0) {
-        u64 cin = 0;
-        if (chunk == 0) {
-            slots[0].incl = cs_eval(agg, 0);
-            __threadfence();
-            st_release(&slots[0].flag, 2u);
-        } else {
-            slots[chunk].agg_h = agg.h;
-            slots[chunk].agg_t = agg.t;
-            __threadfence();
-            st_release(&slots[chunk].flag, 1u);
-            // Walk back, composing aggregates until an inclusive value or a
-            // carry-independent (constant) composition is found.
-            CState acc{0, CS_NEVER};
-            bool acc_id = true;
-            long p = (long)chunk - 1;
-            while (true) {
-                u32 f;
-                int spins = 0;
-                while ((f = ld_acquire(&slots[p].flag)) == 0u) {
-                    if (++spins > LOOKBACK_SPIN_LIMIT) break;
-                    __nanosleep(64);
-                }
-                if (f == 0u) {  // gave up: report, use 0 and finish cleanly
-                    atomicOr(err, 1u);
-                    cin = 0;
-                    break;
-                }
-                if (f == 2u) {
-                    const u64 val = *(volatile u64*)&slots[p].incl;
-                    cin = acc_id ? val : cs_eval(acc, val);
-                    break;
-                }
-                const CState a{*(volatile u64*)&slots[p].agg_h, *(volatile u64*)&slots[p].agg_t};
-                acc = acc_id ? a : cs_then(a, acc);
-                acc_id = false;
-                if (acc.t == CS_NEVER) {  // constant: earlier chunks cannot matter
-                    cin = acc.h;
-                    break;
-                }
-                --p;  // p > 0 here: chunk 0 always publishes inclusive
-            }
-            slots[chunk].incl = cs_eval(agg, cin);
-            __threadfence();
-            st_release(&slots[chunk].flag, 2u);
-        }
-        s_cin = cin;
-    }
+    if (threadIdx.x == 0) s_cin = chunk_lookback(slots, chunk, agg, err);
     __syncthreads();
     const u64 cin_chunk = s_cin;
     const u64 cin = has_ex ? cs_eval(ex, cin_chunk) : cin_chunk;
     group_add_carry<CARRY_G / 2>(lm, cin);
 
-    const u64 lbase = cbase / 2;
+    const u64 lbase = ((u64)chunk * CARRY_CHUNK + (u64)threadIdx.x * CARRY_G) / 2;
     unsigned long long top = 0;
 #pragma unroll
     for (int i = 0; i < CARRY_G / 2; ++i)
@@ -148,30 +183,49 @@ __global__ void __launch_bounds__(CARRY_THREADS, 8) k_carry(const u64* __restric
         for (int i = 0; i < CARRY_G / 2; ++i)
             if (lbase + i < nout) out[lbase + i] = lm[i];
     }
+    // one length update per CTA
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         unsigned long long o = __shfl_xor_sync(0xFFFFFFFFu, top, off);
         top = o > top ? o : top;
     }
-    if ((threadIdx.x & 31) == 0 && top) atomicMax(out_len, top);
+    if ((threadIdx.x & 31) == 0) s_top[warp] = top;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int w = 0; w < CARRY_THREADS / 32; ++w) top = s_top[w] > top ? s_top[w] : top;
+        if (top) atomicMax(out_len, top);
+    }
 }
-
 
 cudaError_t launch_carry(unsigned nchunks, cudaStream_t s, const u64* coef, u32* out, u64 nout,
                          LookbackSlot* slots, u32* ticket, unsigned long long* out_len, u32* err,
                          const ProdJob* jobs, unsigned njobs, u64 points) {
+    if (nchunks == 0 || njobs == 0) return cudaSuccess;
+    // the staging area takes 8 * CARRY_CHUNK bytes per CTA: ask for the
+    // largest shared memory carveout so that CARRY_MIN_CTAS CTAs fit on an SM
+    static const cudaError_t carveout = [] {
+        cudaError_t e = cudaFuncSetAttribute(k_carry<0>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_carry<1>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_carry<2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        return e;
+    }();
+    if (carveout != cudaSuccess) return carveout;
     // scale by points^-1: a shift when points is a power of two (2^(192 - k),
     // k <= 32, is a shift by 160 + (32 - k)), else one multiply
     const dim3 grid(nchunks, njobs);
     if (points <= 1) {
-        k_carry<0><<<grid, CARRY_THREADS, 0, s>>>(coef, out, nout, slots, ticket, out_len, err, jobs, 1, 0);
+        k_carry<0><<<grid, CARRY_THREADS, 0, s>>>(coef, out, nout, nchunks, slots, ticket, out_len, err, jobs, 1, 0);
     } else if ((points & (points - 1)) == 0 && points <= (1ull << 32)) {
         int k = 0;
         while ((1ull << k) < points) ++k;
-        k_carry<1><<<grid, CARRY_THREADS, 0, s>>>(coef, out, nout, slots, ticket, out_len, err, jobs, 1, 192 - k);
+        k_carry<1><<<grid, CARRY_THREADS, 0, s>>>(coef, out, nout, nchunks, slots, ticket, out_len, err, jobs, 1,
+                                                  192 - k);
     } else {
-        k_carry<2><<<grid, CARRY_THREADS, 0, s>>>(coef, out, nout, slots, ticket, out_len, err, jobs, gl_inv(points),
-                                                  -1);
+        k_carry<2><<<grid, CARRY_THREADS, 0, s>>>(coef, out, nout, nchunks, slots, ticket, out_len, err, jobs,
+                                                  gl_inv(points), -1);
     }
     return cudaGetLastError();
 }
