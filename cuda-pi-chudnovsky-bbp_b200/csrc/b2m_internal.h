@@ -58,9 +58,12 @@ std::vector<Plan> plan_candidates(int logn);
 
 // Per-product workspace layout (bytes): two N-element u64 arrays plus the
 // carry scratch (lookback slots, ticket, out_len staging).
+// One chunk's published carry state. `word` is 0 until the chunk publishes;
+// then (value << 2) | state, state 1: aggregate independent of the carry-in
+// (value = its carry-out), 3: aggregate with threshold agg_t (value = the
+// carry-out below it), 2: inclusive carry-out. Carry-outs are below 2^49.
 struct LookbackSlot {
-    u64 agg_h, agg_t, incl;
-    u32 flag, pad;
+    u64 word, agg_t;
 };
 uint64_t workspace_bytes_for(int logn);
 

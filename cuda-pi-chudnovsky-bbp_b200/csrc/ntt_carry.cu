@@ -14,7 +14,8 @@ namespace b2m {
 // Carry: coefficients (natural order, N of them) -> nout u32 limbs.
 // One CTA per chunk of 4096 coefficients, chunks claimed in launch order by
 // ticket so that every chunk a CTA waits for belongs to a CTA that is already
-// running and publishes its aggregate without waiting. Waits are bounded:
+// running and publishes its aggregate without waiting. Warp 0 resolves the
+// chunk's carry-in, 32 predecessors per round trip. Waits are bounded:
 // after ~2^22 polls the kernel flags *err and carries on with a wrong carry
 // (the host turns the flag into B2M_ERR_DEVICE_TIMEOUT).
 //
@@ -24,15 +25,15 @@ namespace b2m {
 // own 128 contiguous bytes read directly would touch 32 cache lines per warp
 // load instruction, eight times the L1 wavefronts of the coalesced read.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ u32 ld_acquire(const u32* p) {
-    u32 v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+__device__ __forceinline__ u64 ld_acquire(const u64* p) {
+    u64 v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
-// Release store: the thread's earlier writes (the slot's values) are visible
-// to any thread that reads this flag with ld_acquire.
-__device__ __forceinline__ void st_release(u32* p, u32 v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+// Release store: the thread's earlier writes (the slot's threshold) are
+// visible to any thread that reads this word with ld_acquire.
+__device__ __forceinline__ void st_release(u64* p, u64 v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 constexpr int LOOKBACK_SPIN_LIMIT = 1 << 22;
@@ -68,52 +69,68 @@ __device__ __forceinline__ void load_chunk(const u64* __restrict__ coef, u64 wba
     }
 }
 
-// Thread 0: publish chunk `chunk`'s aggregate, then walk back composing
-// predecessors' aggregates until an inclusive value or a carry-independent
-// (constant) composition is found; publish the inclusive value and return
-// the chunk's carry-in.
-__device__ __forceinline__ u64 chunk_lookback(LookbackSlot* slots, u32 chunk, CState agg, u32* err) {
+constexpr u64 SLOT_CONST = 1, SLOT_INCL = 2, SLOT_AGG = 3;
+
+__device__ __forceinline__ CState cs_shfl(CState f, int src) {
+    return {__shfl_sync(0xFFFFFFFFu, f.h, src), __shfl_sync(0xFFFFFFFFu, f.t, src)};
+}
+
+// Warp 0 (all lanes): publish chunk `chunk`'s aggregate, then resolve its
+// carry-in. Each round reads the slots of the 32 nearest unresolved
+// predecessors at once (lane i: chunk base - i); the nearest slot holding a
+// constant aggregate or an inclusive value ends the walk, the aggregates in
+// front of it are composed onto it. A round with 32 thresholded aggregates
+// composes them all and moves 32 chunks further back. Returns the carry-in
+// on every lane; the inclusive value is published by the caller.
+__device__ __forceinline__ u64 warp_lookback(LookbackSlot* slots, u32 chunk, CState agg, u32* err) {
+    const int lane = threadIdx.x & 31;
     if (chunk == 0) {
-        slots[0].incl = cs_eval(agg, 0);
-        st_release(&slots[0].flag, 2u);
+        if (lane == 0) st_release(&slots[0].word, (cs_eval(agg, 0) << 2) | SLOT_INCL);
         return 0;
     }
-    slots[chunk].agg_h = agg.h;
-    slots[chunk].agg_t = agg.t;
-    st_release(&slots[chunk].flag, 1u);
-    u64 cin = 0;
-    CState acc{0, CS_NEVER};
+    if (lane == 0) {
+        if (agg.t != CS_NEVER) slots[chunk].agg_t = agg.t;
+        st_release(&slots[chunk].word, (agg.h << 2) | (agg.t == CS_NEVER ? SLOT_CONST : SLOT_AGG));
+    }
+    CState acc{0, CS_NEVER};  // composition of the predecessors passed so far (nearest applied last)
     bool acc_id = true;
-    long p = (long)chunk - 1;
+    long base = (long)chunk - 1;
+    int spins = 0;
     while (true) {
-        u32 f;
-        int spins = 0;
-        while ((f = ld_acquire(&slots[p].flag)) == 0u) {
-            if (++spins > LOOKBACK_SPIN_LIMIT) break;
+        const long p = base - lane;
+        u64 w = SLOT_INCL;  // before chunk 0: carry 0
+        unsigned need;
+        int f;
+        while (true) {
+            if (p >= 0) w = ld_acquire(&slots[p].word);
+            const unsigned stop = __ballot_sync(0xFFFFFFFFu, (w & 3) == SLOT_CONST || (w & 3) == SLOT_INCL);
+            const unsigned pub = __ballot_sync(0xFFFFFFFFu, (w & 3) != 0);
+            f = stop ? __ffs(stop) - 1 : 31;  // lanes 0..f must be published
+            need = f == 31 ? 0xFFFFFFFFu : ((2u << f) - 1);
+            if ((pub & need) == need) break;
+            if (++spins > LOOKBACK_SPIN_LIMIT) {  // gave up: report, use 0 and finish cleanly
+                if (lane == 0) atomicOr(err, 1u);
+                return 0;
+            }
             __nanosleep(64);
         }
-        if (f == 0u) {  // gave up: report, use 0 and finish cleanly
-            atomicOr(err, 1u);
-            cin = 0;
-            break;
+        CState mine{w >> 2, CS_NEVER};
+        if ((w & 3) == SLOT_AGG) mine.t = *(volatile u64*)&slots[p].agg_t;
+        const unsigned stop = __ballot_sync(0xFFFFFFFFu, (w & 3) != SLOT_AGG);
+        if (stop & need) {
+            // lane f is constant or inclusive: evaluate lanes f-1 .. 0 on its value
+            u64 x = __shfl_sync(0xFFFFFFFFu, mine.h, f);
+            for (int k = f - 1; k >= 0; --k) x = cs_eval(cs_shfl(mine, k), x);
+            return acc_id ? x : cs_eval(acc, x);
         }
-        if (f == 2u) {
-            const u64 val = *(volatile u64*)&slots[p].incl;
-            cin = acc_id ? val : cs_eval(acc, val);
-            break;
-        }
-        const CState a{*(volatile u64*)&slots[p].agg_h, *(volatile u64*)&slots[p].agg_t};
-        acc = acc_id ? a : cs_then(a, acc);
+        // 32 thresholded aggregates: compose them (lane 31 applies first)
+        CState blk = cs_shfl(mine, 31);
+        for (int k = 30; k >= 0; --k) blk = cs_then(blk, cs_shfl(mine, k));
+        acc = acc_id ? blk : cs_then(blk, acc);
         acc_id = false;
-        if (acc.t == CS_NEVER) {  // constant: earlier chunks cannot matter
-            cin = acc.h;
-            break;
-        }
-        --p;  // p > 0 here: chunk 0 always publishes inclusive
+        if (acc.t == CS_NEVER) return acc.h;  // constant: earlier chunks cannot matter
+        base -= 32;
     }
-    slots[chunk].incl = cs_eval(agg, cin);
-    st_release(&slots[chunk].flag, 2u);
-    return cin;
 }
 
 // SC: how the coefficients are scaled by N^-1 before the carry -- 0 not at all
@@ -138,6 +155,7 @@ __global__ void __launch_bounds__(CARRY_THREADS, CARRY_MIN_CTAS)
     __shared__ u32 s_chunk;
     __shared__ u64 s_cin;
     __shared__ unsigned long long s_top[CARRY_THREADS / 32];
+    __shared__ u64 s_lasth[CARRY_THREADS / 32];
     __shared__ CState s_ws[CARRY_THREADS / 32 + 1];
     if (threadIdx.x == 0) s_chunk = atomicAdd(ticket, 1u);
     __syncthreads();
@@ -159,13 +177,52 @@ __global__ void __launch_bounds__(CARRY_THREADS, CARRY_MIN_CTAS)
     }
     u32 lm[CARRY_G / 2];
     const CState st = group_carry<CARRY_G>(cf, lm);
-    bool has_ex;
-    CState agg;
-    const CState ex = block_scan_carry(st, &has_ex, &agg, s_ws);
-    if (threadIdx.x == 0) s_cin = chunk_lookback(slots, chunk, agg, err);
-    __syncthreads();
-    const u64 cin_chunk = s_cin;
-    const u64 cin = has_ex ? cs_eval(ex, cin_chunk) : cin_chunk;
+    // park the limbs in the thread's own (already read) staging slots while
+    // warp 0 walks back, so that the walk has the registers to itself; slot
+    // i ^ (lane % 8) of the lane's eight keeps a quarter warp conflict-free
+    const int lane = threadIdx.x & 31;
+    {
+        uint4* mine = reinterpret_cast<uint4*>(s_stage[warp] + lane * (CARRY_G / 2));
+#pragma unroll
+        for (int i = 0; i < CARRY_G / 8; ++i)
+            mine[i ^ (lane & 7)] = make_uint4(lm[4 * i], lm[4 * i + 1], lm[4 * i + 2], lm[4 * i + 3]);
+    }
+    const u64 h_before = __shfl_up_sync(0xFFFFFFFFu, st.h, 1);
+    if (lane == 31) s_lasth[warp] = st.h;
+    u64 cin;
+    if (!__syncthreads_or(st.t != CS_NEVER)) {
+        // Every group's carry-out is independent of its carry-in (the usual
+        // case): group k > 0 takes group k-1's carry-out, no scan needed, and
+        // only thread 0 waits for the chunk's carry-in. The chunk's aggregate
+        // is constant, which is all a successor needs.
+        const CState agg{s_lasth[CARRY_THREADS / 32 - 1], CS_NEVER};
+        cin = lane > 0 ? h_before : (warp > 0 ? s_lasth[warp - 1] : 0);
+        if (warp == 0) {
+            const u64 c = warp_lookback(slots, chunk, agg, err);
+            if (lane == 0) cin = c;
+        }
+    } else {
+        bool has_ex;
+        CState agg;
+        const CState ex = block_scan_carry(st, &has_ex, &agg, s_ws);
+        if (warp == 0) {
+            const u64 c = warp_lookback(slots, chunk, agg, err);
+            if (threadIdx.x == 0) s_cin = c;
+        }
+        __syncthreads();
+        const u64 cin_chunk = s_cin;
+        // successors waiting on a thresholded aggregate need the inclusive value
+        if (threadIdx.x == 0) st_release(&slots[chunk].word, (cs_eval(agg, cin_chunk) << 2) | SLOT_INCL);
+        cin = has_ex ? cs_eval(ex, cin_chunk) : cin_chunk;
+    }
+    {
+        const uint4* mine = reinterpret_cast<const uint4*>(s_stage[warp] + lane * (CARRY_G / 2));
+#pragma unroll
+        for (int i = 0; i < CARRY_G / 8; ++i) {
+            const uint4 q = mine[i ^ (lane & 7)];
+            lm[4 * i] = q.x, lm[4 * i + 1] = q.y, lm[4 * i + 2] = q.z, lm[4 * i + 3] = q.w;
+        }
+    }
     group_add_carry<CARRY_G / 2>(lm, cin);
 
     const u64 lbase = ((u64)chunk * CARRY_CHUNK + (u64)threadIdx.x * CARRY_G) / 2;
