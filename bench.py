@@ -337,7 +337,10 @@ def run_ours(args) -> None:
                     "all_products_residue_checked_ok": v["all_products_residue_checked_ok"]}
 
         at_cfg = summary(measure_serve(rk, args))
-        serve = {"at_config_rate": at_cfg}
+        serve = {"at_config_rate": at_cfg,
+                 # the same size mix submitted all at once: what the server
+                 # and device can complete, against the configured offer
+                 "closed_loop_capacity": serve_capacity(rk, args)}
         # A sustainable rate: when the configured rate overloads the server
         # (its queue grows), 75% of the rate it actually served; otherwise the
         # configured rate itself is sustainable and is not repeated.
