@@ -51,6 +51,53 @@ def test_edge_sizes_against_oracle(b2m_gpu, na, nb, kind):
     assert p.size == q.size and np.array_equal(p, q)
 
 
+def runs_operand(seed, n):
+    """n limbs in runs of 0xFFFFFFFF, zero and random limbs, run lengths
+    1..6000 (so runs cross the carry kernel's 2048-limb chunks), top limb
+    non-zero."""
+    rng = np.random.default_rng(seed)
+    out = np.empty(n, np.uint32)
+    i, run = 0, int(rng.integers(0, 3))
+    while i < n:
+        k = min(n - i, int(rng.integers(1, 6001)))
+        kind = run % 3  # all ones, zeros, random in turn
+        out[i:i + k] = (0xFFFFFFFF if kind == 0 else 0) if kind < 2 else rng.integers(0, 1 << 32, k, np.uint64)
+        i += k
+        run += 1
+    out[-1] |= 1
+    return out
+
+
+def ones_plus(n, m):
+    """(2^(32n) - 1, 2^(32m) + 1): their product has 0xFFFFFFFF runs of n - m
+    limbs between sparse limbs, so whole carry chunks are all ones while
+    their neighbours are not."""
+    a = np.full(n, 0xFFFFFFFF, np.uint32)
+    b = np.zeros(m + 1, np.uint32)
+    b[0] = b[m] = 1
+    return a, b
+
+
+@pytest.mark.parametrize("na,nb", [(1 << 14, 1 << 14), (1 << 16, 1 << 15), (1 << 17, 1 << 17), (50000, 70001),
+                                   (262144, 8192)])
+def test_structured_runs_against_oracle(b2m_gpu, na, nb):
+    """Carry stress: operands made of long runs, so that some chunks of the
+    carry resolve by the scan-free path, others by the full scan, and the
+    lookback crosses both kinds of aggregate (include/ntt.h:70-91)."""
+    a, b = runs_operand(na, na), runs_operand(nb + 1, nb)
+    p = b2m_gpu.mul_ntt_cuda(a, b)
+    q = oracle.mul_port(a, b)
+    assert p.size == q.size and np.array_equal(p, q)
+
+
+@pytest.mark.parametrize("n,m", [(20000, 3000), (70000, 65536), (131072, 1), (150000, 40000)])
+def test_all_ones_run_products_against_oracle(b2m_gpu, n, m):
+    a, b = ones_plus(n, m)
+    p = b2m_gpu.mul_ntt_cuda(a, b)
+    q = oracle.mul_port(a, b)
+    assert p.size == q.size and np.array_equal(p, q)
+
+
 @pytest.mark.parametrize("entry", (load("sweep_small.json") or {"products": []})["products"],
                          ids=lambda e: e["name"])
 def test_sweep_against_reference_hashes(b2m_gpu, entry):
