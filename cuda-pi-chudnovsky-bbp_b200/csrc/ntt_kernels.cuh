@@ -53,6 +53,24 @@ __device__ __forceinline__ u64 digit_of(const u32* __restrict__ limbs, u64 ndig,
     return (n & 1) ? (u64)(w >> 16) : (u64)(w & 0xFFFFu);
 }
 
+// Digits of K consecutive rows of a thread's column into shared memory. A
+// thread's elements gi0 + k*gstep share the parity of gi0 (gstep is even), so
+// each takes the same half of its limb; when the last of them is below ndig
+// (every tile but the operand's last) no element needs the bounds check.
+template <int K, class G>
+__device__ __forceinline__ void load_digits(u64* sm, const G& gp, const u32* __restrict__ limbs, u64 ndig) {
+    if (!(gp.gstep & 1) && gp.gi0 + (u64)(K - 1) * gp.gstep < ndig) {
+        const u32* lp = limbs + (gp.gi0 >> 1);
+        const u64 ls = gp.gstep >> 1;
+        const u32 sh = (u32)(gp.gi0 & 1) << 4;
+#pragma unroll
+        for (int k = 0; k < K; ++k) sm[gp.sa0 + G::soff(k)] = (u64)((__ldg(lp + k * ls) >> sh) & 0xFFFFu);
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; ++k) sm[gp.sa0 + G::soff(k)] = digit_of(limbs, ndig, gp.gi0 + k * gp.gstep);
+    }
+}
+
 // Column-mapped pass geometry (first, middle and non-last inverse passes).
 // The tile is rows [0, R) of columns [g0, g0 + C), C <= S, so all of it lies in
 // one sub-problem b = g0 >> logS. Thread t owns column col = t mod C and rows
@@ -124,13 +142,18 @@ k_fwd_first(const u32* __restrict__ limbs, u64 ndig, u64* __restrict__ out, int 
         out = operand ? J.bufB : J.bufA;
     }
     const G gp(logS, logM);
-#pragma unroll
-    for (int k = 0; k < G::PER; ++k) sm[gp.sa0 + G::soff(k)] = digit_of(limbs, ndig, gp.gi0 + k * gp.gstep);
-    __syncthreads();
     // The digits fill at most half of the transform for almost every product
-    // (N >= 2 (na + nb)): rows [R/2, R) of every column are then zero.
-    if (2 * ndig <= (1ull << logM)) tile_fwd<TL, (Steps<LOGR>::G >= 2), true>(sm, tw.dtw);
-    else tile_fwd<TL>(sm, tw.dtw);
+    // (N >= 2 (na + nb)): rows [R/2, R) of every column are then zero, and
+    // the half-zero tile transform neither reads nor needs them.
+    if (2 * ndig <= (1ull << logM)) {
+        load_digits<G::PER / 2>(sm, gp, limbs, ndig);  // rows row0 + k*DR < R/2
+        __syncthreads();
+        tile_fwd<TL, (Steps<LOGR>::G >= 2), true>(sm, tw.dtw);
+    } else {
+        load_digits<G::PER>(sm, gp, limbs, ndig);
+        __syncthreads();
+        tile_fwd<TL>(sm, tw.dtw);
+    }
     if (ttab) {
 #pragma unroll
         for (int k = 0; k < G::PER; ++k)
