@@ -46,6 +46,13 @@ __device__ __forceinline__ void cp_async8(u64* smem_dst, const u64* gsrc) {
 __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
+__device__ __forceinline__ void cp_async16(u64* smem_dst, const u64* gsrc) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ ulonglong2 ld2(const u64* p) { return *reinterpret_cast<const ulonglong2*>(p); }
+__device__ __forceinline__ void st2(u64* p, ulonglong2 v) { *reinterpret_cast<ulonglong2*>(p) = v; }
+__device__ __forceinline__ ulonglong2 ldg2(const u64* p) { return __ldg(reinterpret_cast<const ulonglong2*>(p)); }
 
 __device__ __forceinline__ u64 digit_of(const u32* __restrict__ limbs, u64 ndig, u64 n) {
     if (n >= ndig) return 0;
@@ -68,6 +75,28 @@ __device__ __forceinline__ void load_digits(u64* sm, const G& gp, const u32* __r
     } else {
 #pragma unroll
         for (int k = 0; k < K; ++k) sm[gp.sa0 + G::soff(k)] = digit_of(limbs, ndig, gp.gi0 + k * gp.gstep);
+    }
+}
+
+// Digits of K chunks of column pairs (ColPair): digit pair n, n+1 (n even)
+// is one u32 limb, and n < ndig (ndig even) covers both digits.
+template <int K, class P>
+__device__ __forceinline__ void load_digit_pairs(u64* sm, const P& pp, const u32* __restrict__ limbs, u64 ndig) {
+    if (pp.gi0 + (u64)(K - 1) * pp.gstep < ndig) {
+        const u32* lp = limbs + (pp.gi0 >> 1);
+        const u64 ls = pp.gstep >> 1;
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const u32 w = __ldg(lp + j * ls);
+            st2(sm + pp.sa0 + P::soff(j), make_ulonglong2(w & 0xFFFFu, w >> 16));
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const u64 n = pp.gi0 + j * pp.gstep;
+            const u32 w = n < ndig ? __ldg(limbs + (n >> 1)) : 0u;
+            st2(sm + pp.sa0 + P::soff(j), make_ulonglong2(w & 0xFFFFu, w >> 16));
+        }
     }
 }
 
@@ -103,6 +132,32 @@ struct ColPass {
     // shared-address offset and bit-reversed row part of element k
     static constexpr int soff(int k) { return (k * DR + ((k * DR) >> 6)) << TL::LC; }
     static constexpr u32 fk(int k) { return (u32)brev_c(k * DR, TL::LR); }
+};
+
+// The same tile moved as 16-byte column pairs: thread t moves columns
+// 2*(t mod C/2) and the next one of rows r0 + j*DR2 (r0 = t / (C/2) < DR2,
+// j < 8). Pairs start at even columns of a sub-problem of stride S >= C, so
+// the global, table and shared addresses are 16-byte aligned, and r0 < DR2
+// with DR2 a power of two keeps the padded shared offsets linear in j.
+template <class TL>
+struct ColPair {
+    static constexpr int CP = TL::C / 2;
+    static constexpr int DR2 = TL::T / CP;
+    static constexpr int PER = (TL::R * CP) / TL::T;
+    static_assert(TL::LC >= 1 && PER == 8, "column pairs: eight 16-byte chunks per thread");
+    int sa0;
+    u64 gi0, gstep, ti0;
+    __device__ __forceinline__ explicit ColPair(int logS) {
+        const int cp = (int)threadIdx.x & (CP - 1);
+        const int r0 = (int)threadIdx.x / CP;
+        sa0 = TL::saddr(r0, 2 * cp);
+        const u64 g = ((u64)blockIdx.x << TL::LC) + 2 * cp;
+        const u64 c = g & ((1ull << logS) - 1);
+        gi0 = ((g >> logS) << (TL::LR + logS)) + ((u64)r0 << logS) + c;
+        ti0 = ((u64)r0 << logS) + c;
+        gstep = (u64)DR2 << logS;
+    }
+    static constexpr int soff(int j) { return (j * DR2 + ((j * DR2) >> 6)) << TL::LC; }
 };
 
 // Row-mapped (contiguous) tile of the last forward / first inverse pass:
@@ -144,15 +199,32 @@ k_fwd_first(const u32* __restrict__ limbs, u64 ndig, u64* __restrict__ out, int 
     const G gp(logS, logM);
     // The digits fill at most half of the transform for almost every product
     // (N >= 2 (na + nb)): rows [R/2, R) of every column are then zero, and
-    // the half-zero tile transform neither reads nor needs them.
+    // the half-zero tile transform neither reads nor needs them. Tiles of
+    // two or more columns move digit pairs (one limb each).
     if (2 * ndig <= (1ull << logM)) {
-        load_digits<G::PER / 2>(sm, gp, limbs, ndig);  // rows row0 + k*DR < R/2
+        if constexpr (TL::LC >= 1) load_digit_pairs<4>(sm, ColPair<TL>(logS), limbs, ndig);  // rows < R/2
+        else load_digits<G::PER / 2>(sm, gp, limbs, ndig);  // rows row0 + k*DR < R/2
         __syncthreads();
         tile_fwd<TL, (Steps<LOGR>::G >= 2), true>(sm, tw.dtw);
     } else {
-        load_digits<G::PER>(sm, gp, limbs, ndig);
+        if constexpr (TL::LC >= 1) load_digit_pairs<8>(sm, ColPair<TL>(logS), limbs, ndig);
+        else load_digits<G::PER>(sm, gp, limbs, ndig);
         __syncthreads();
         tile_fwd<TL>(sm, tw.dtw);
+    }
+    if constexpr (TL::LC >= 1) {
+        if (ttab) {
+            const ColPair<TL> pp(logS);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                ulonglong2 v = ld2(sm + pp.sa0 + ColPair<TL>::soff(j));
+                const ulonglong2 t = ldg2(ttab + pp.ti0 + j * pp.gstep);
+                v.x = gl_mul(v.x, t.x);
+                v.y = gl_mul(v.y, t.y);
+                st2(out + pp.gi0 + j * pp.gstep, v);
+            }
+            return;
+        }
     }
     if (ttab) {
 #pragma unroll
@@ -180,11 +252,31 @@ k_fwd_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const u64* _
     if (jobs) buf = operand ? jobs[blockIdx.y].bufB : jobs[blockIdx.y].bufA;
     buf += blockIdx.z * zstride;  // sub-transform of a radix-3 plan
     const G gp(logS, logM);
+    if constexpr (TL::LC >= 1) {
+        const ColPair<TL> pp(logS);
 #pragma unroll
-    for (int k = 0; k < G::PER; ++k) cp_async8(sm + gp.sa0 + G::soff(k), buf + gp.gi0 + k * gp.gstep);
+        for (int j = 0; j < 8; ++j) cp_async16(sm + pp.sa0 + ColPair<TL>::soff(j), buf + pp.gi0 + j * pp.gstep);
+    } else {
+#pragma unroll
+        for (int k = 0; k < G::PER; ++k) cp_async8(sm + gp.sa0 + G::soff(k), buf + gp.gi0 + k * gp.gstep);
+    }
     cp_async_wait_all();
     __syncthreads();
     tile_fwd<TL>(sm, tw.dtw);
+    if constexpr (TL::LC >= 1) {
+        if (ttab) {
+            const ColPair<TL> pp(logS);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                ulonglong2 v = ld2(sm + pp.sa0 + ColPair<TL>::soff(j));
+                const ulonglong2 t = ldg2(ttab + pp.ti0 + j * pp.gstep);
+                v.x = gl_mul(v.x, t.x);
+                v.y = gl_mul(v.y, t.y);
+                st2(buf + pp.gi0 + j * pp.gstep, v);
+            }
+            return;
+        }
+    }
     if (ttab) {
 #pragma unroll
         for (int k = 0; k < G::PER; ++k)
@@ -215,31 +307,60 @@ k_inv_mid(u64* __restrict__ buf, int logS, int logM, RootTables tw, const u64* _
     const G gp(logS, logM);
     // the tile arrives by asynchronous copies while the twiddles load; each
     // thread then multiplies the elements it copied
+    bool paired = false;
+    if constexpr (TL::LC >= 1) {
+        if (ttab) {
+            paired = true;
+            const ColPair<TL> pp(logS);
 #pragma unroll
-    for (int k = 0; k < G::PER; ++k) cp_async8(sm + gp.sa0 + G::soff(k), buf + gp.gi0 + k * gp.gstep);
-    if (ttab) {
-        u64 t[G::PER];
+            for (int j = 0; j < 8; ++j) cp_async16(sm + pp.sa0 + ColPair<TL>::soff(j), buf + pp.gi0 + j * pp.gstep);
+            ulonglong2 t[8];
 #pragma unroll
-        for (int k = 0; k < G::PER; ++k) t[k] = __ldg(ttab + gp.ti0 + k * gp.gstep);
-        cp_async_wait_all();
+            for (int j = 0; j < 8; ++j) t[j] = ldg2(ttab + pp.ti0 + j * pp.gstep);
+            cp_async_wait_all();
 #pragma unroll
-        for (int k = 0; k < G::PER; ++k) {
-            u64& v = sm[gp.sa0 + G::soff(k)];
-            v = gl_mul(v, t[k]);
+            for (int j = 0; j < 8; ++j) {
+                u64* p = sm + pp.sa0 + ColPair<TL>::soff(j);
+                ulonglong2 v = ld2(p);
+                v.x = gl_mul(v.x, t[j].x);
+                v.y = gl_mul(v.y, t[j].y);
+                st2(p, v);
+            }
         }
-    } else {
-        cp_async_wait_all();
+    }
+    if (!paired) {
 #pragma unroll
-        for (int k = 0; k < G::PER; ++k) {
-            const u32 e = gp.e0 + G::fk(k) * gp.ec;
-            u64& v = sm[gp.sa0 + G::soff(k)];
-            if (e) v = gl_mul(v, uroot(0u - e, tw.u1, tw.u2));
+        for (int k = 0; k < G::PER; ++k) cp_async8(sm + gp.sa0 + G::soff(k), buf + gp.gi0 + k * gp.gstep);
+        if (ttab) {
+            u64 t[G::PER];
+#pragma unroll
+            for (int k = 0; k < G::PER; ++k) t[k] = __ldg(ttab + gp.ti0 + k * gp.gstep);
+            cp_async_wait_all();
+#pragma unroll
+            for (int k = 0; k < G::PER; ++k) {
+                u64& v = sm[gp.sa0 + G::soff(k)];
+                v = gl_mul(v, t[k]);
+            }
+        } else {
+            cp_async_wait_all();
+#pragma unroll
+            for (int k = 0; k < G::PER; ++k) {
+                const u32 e = gp.e0 + G::fk(k) * gp.ec;
+                u64& v = sm[gp.sa0 + G::soff(k)];
+                if (e) v = gl_mul(v, uroot(0u - e, tw.u1, tw.u2));
+            }
         }
     }
     __syncthreads();
     tile_inv<TL>(sm, tw.dtw);
+    if constexpr (TL::LC >= 1) {
+        const ColPair<TL> pp(logS);
 #pragma unroll
-    for (int k = 0; k < G::PER; ++k) buf[gp.gi0 + k * gp.gstep] = sm[gp.sa0 + G::soff(k)];
+        for (int j = 0; j < 8; ++j) st2(buf + pp.gi0 + j * pp.gstep, ld2(sm + pp.sa0 + ColPair<TL>::soff(j)));
+    } else {
+#pragma unroll
+        for (int k = 0; k < G::PER; ++k) buf[gp.gi0 + k * gp.gstep] = sm[gp.sa0 + G::soff(k)];
+    }
 }
 
 // Last forward pass of operand A (S = 1: each column is a contiguous
