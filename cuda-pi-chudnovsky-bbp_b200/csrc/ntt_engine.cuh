@@ -90,6 +90,10 @@ constexpr int brev_c(int v, int bits) {
 
 enum { MAP_COL = 0, MAP_ROW = 1 };
 
+// Two adjacent u64 (16-byte aligned) in one access.
+__device__ __forceinline__ ulonglong2 ld2(const u64* p) { return *reinterpret_cast<const ulonglong2*>(p); }
+__device__ __forceinline__ void st2(u64* p, ulonglong2 v) { *reinterpret_cast<ulonglong2*>(p) = v; }
+
 // Tile geometry, all compile-time: R = 2^LOGR rows by C = 2^LOGC columns,
 // T = max(1, R*C/16) threads, so every radix-8 level is two 8-point tasks per
 // thread and every load or store loop is 16 elements per thread.
@@ -106,6 +110,14 @@ struct Tile {
     static constexpr int RP = R + (R >> 6);
     static constexpr int LOGT = LOGR + LOGC >= 4 ? LOGR + LOGC - 4 : 0;
     static constexpr int T = 1 << LOGT;
+    // Column-mapped tiles of two or more columns run their inverse 8-point
+    // tasks in pairs of adjacent columns: the two tasks' elements are
+    // adjacent in shared memory (16-byte aligned: even column, rows of
+    // C >= 2 elements), so each pair of elements is one 16-byte access, and
+    // a twiddle that depends only on the row serves both columns. Forward
+    // tasks stay single: with their eight specialised level-1 bodies the
+    // paired form measured slower (more code, register spills).
+    static constexpr bool PAIR = MAP == MAP_COL && LOGC >= 1 && LOGR + LOGC >= 5;
 
     static constexpr int pad(int row) { return row + (row >> 6); }
     __device__ __forceinline__ static int saddr(int row, int col) {
@@ -165,6 +177,42 @@ struct Steps {
 template <class TL, int A, bool INV, bool ZH = false>
 __device__ __forceinline__ void lead_step(u64* sm, const u64* __restrict__ dtw) {
     constexpr int E = 1 << A, R = TL::R, LOGJ = TL::LR - A, JW = R >> A;
+    if constexpr (TL::PAIR && INV) {
+        for_tasks<(JW << (TL::LC - 1)), TL::T>([&](int p) {
+            const int col = (p << 1) & (TL::C - 1), j = (p << 1) >> TL::LC;
+            u64 x[E], y[E];
+            u64* ptr = sm + TL::saddr(j, col);
+            constexpr int st = TL::template step<JW>();
+#pragma unroll
+            for (int m = 0; m < (ZH ? E / 2 : E); ++m) {
+                const ulonglong2 v = ld2(ptr + m * st);
+                x[m] = v.x;
+                y[m] = v.y;
+            }
+            if (!INV) {
+                dft_fwd<E, ZH>(x);
+                dft_fwd<E, ZH>(y);
+#pragma unroll
+                for (int i = 1; i < E; ++i) {
+                    const u64 w = __ldg(dtw + R + ((j * brev_c(i, A)) & (R - 1)));
+                    x[i] = gl_mul(x[i], w);
+                    y[i] = gl_mul(y[i], w);
+                }
+            } else {
+#pragma unroll
+                for (int i = 1; i < E; ++i) {
+                    const u64 w = __ldg(dtw + R + ((R - ((j * brev_c(i, A)) & (R - 1))) & (R - 1)));
+                    x[i] = gl_mul(x[i], w);
+                    y[i] = gl_mul(y[i], w);
+                }
+                dft_inv<E>(x);
+                dft_inv<E>(y);
+            }
+#pragma unroll
+            for (int m = 0; m < E; ++m) st2(ptr + m * st, make_ulonglong2(x[m], y[m]));
+        });
+        return;
+    }
     for_tasks<(JW << TL::LC), TL::T>([&](int q) {
         int col, j;
         if (TL::MAPK == MAP_COL) {
@@ -255,6 +303,36 @@ __device__ __forceinline__ void group64(u64* sm, const u64* __restrict__ dtw) {
     constexpr int NI = 1 << LOGNI;
     constexpr int TASKS = NI << 3;
     auto level1 = [&]() {
+        if constexpr (TL::PAIR && INV) {
+            for_tasks<TASKS / 2, TL::T>([&](int p) {
+                const int u1 = p >> (LOGNI - 1);
+                int col, blk, j;
+                TL::template decode<LOGJ>((p & (NI / 2 - 1)) << 1, col, blk, j);
+                u64* ptr = sm + TL::saddr(blk * L + j + u1 * JW, col);
+                constexpr int st = TL::template step<8 * JW>();
+                u64 x[8], y[8];
+#pragma unroll
+                for (int m = 0; m < (ZH ? 4 : 8); ++m) {
+                    const ulonglong2 v = ld2(ptr + m * st);
+                    x[m] = v.x;
+                    y[m] = v.y;
+                }
+                if (!INV) {
+                    dft_fwd<8, ZH>(x);
+                    dft_fwd<8, ZH>(y);
+                    level1_twiddle<false, RT>(x, u1);
+                    level1_twiddle<false, RT>(y, u1);
+                } else {
+                    level1_twiddle<true, RT>(x, u1);
+                    level1_twiddle<true, RT>(y, u1);
+                    dft_inv<8>(x);
+                    dft_inv<8>(y);
+                }
+#pragma unroll
+                for (int m = 0; m < 8; ++m) st2(ptr + m * st, make_ulonglong2(x[m], y[m]));
+            });
+            return;
+        }
         for_tasks<TASKS, TL::T>([&](int q) {
             const int u1 = q >> LOGNI;
             int col, blk, j;
@@ -276,6 +354,51 @@ __device__ __forceinline__ void group64(u64* sm, const u64* __restrict__ dtw) {
         });
     };
     auto level2 = [&]() {
+        if constexpr (TL::PAIR && INV) {
+            for_tasks<TASKS / 2, TL::T>([&](int p) {
+                const int i1 = p >> (LOGNI - 1);
+                int col, blk, j;
+                TL::template decode<LOGJ>((p & (NI / 2 - 1)) << 1, col, blk, j);
+                u64* ptr = sm + TL::saddr(blk * L + j + i1 * 8 * JW, col);
+                constexpr int st = TL::template step<JW>();
+                const int k1 = brev_c(i1, 3);
+                u64 x[8], y[8];
+#pragma unroll
+                for (int m = 0; m < 8; ++m) {
+                    const ulonglong2 v = ld2(ptr + m * st);
+                    x[m] = v.x;
+                    y[m] = v.y;
+                }
+                if (!INV) {
+                    dft_fwd<8>(x);
+                    dft_fwd<8>(y);
+                    if (L > 64) {
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) {
+                            const int k = k1 + 8 * brev_c(i, 3);
+                            const u64 w = __ldg(dtw + L + ((j * k) & (L - 1)));
+                            x[i] = gl_mul(x[i], w);
+                            y[i] = gl_mul(y[i], w);
+                        }
+                    }
+                } else {
+                    if (L > 64) {
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) {
+                            const int k = k1 + 8 * brev_c(i, 3);
+                            const u64 w = __ldg(dtw + L + ((L - ((j * k) & (L - 1))) & (L - 1)));
+                            x[i] = gl_mul(x[i], w);
+                            y[i] = gl_mul(y[i], w);
+                        }
+                    }
+                    dft_inv<8>(x);
+                    dft_inv<8>(y);
+                }
+#pragma unroll
+                for (int m = 0; m < 8; ++m) st2(ptr + m * st, make_ulonglong2(x[m], y[m]));
+            });
+            return;
+        }
         for_tasks<TASKS, TL::T>([&](int q) {
             const int i1 = q >> LOGNI;
             int col, blk, j;
@@ -324,6 +447,30 @@ __device__ __forceinline__ void group64(u64* sm, const u64* __restrict__ dtw) {
 template <class TL, bool INV>
 __device__ __forceinline__ void lone8(u64* sm) {
     constexpr int LOGNB = TL::LR - 3;
+    if constexpr (TL::PAIR && INV) {
+        for_tasks<(1 << (LOGNB + TL::LC - 1)), TL::T>([&](int p) {
+            const int col = (p << 1) & (TL::C - 1), blk = (p << 1) >> TL::LC;
+            u64* ptr = sm + TL::saddr(blk * 8, col);
+            constexpr int st = TL::template step<1>();
+            u64 x[8], y[8];
+#pragma unroll
+            for (int m = 0; m < 8; ++m) {
+                const ulonglong2 v = ld2(ptr + m * st);
+                x[m] = v.x;
+                y[m] = v.y;
+            }
+            if (!INV) {
+                dft_fwd<8>(x);
+                dft_fwd<8>(y);
+            } else {
+                dft_inv<8>(x);
+                dft_inv<8>(y);
+            }
+#pragma unroll
+            for (int m = 0; m < 8; ++m) st2(ptr + m * st, make_ulonglong2(x[m], y[m]));
+        });
+        return;
+    }
     for_tasks<(1 << (LOGNB + TL::LC)), TL::T>([&](int q) {
         int col, blk;
         if (TL::MAPK == MAP_COL) {

@@ -50,8 +50,6 @@ __device__ __forceinline__ void cp_async16(u64* smem_dst, const u64* gsrc) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
 }
-__device__ __forceinline__ ulonglong2 ld2(const u64* p) { return *reinterpret_cast<const ulonglong2*>(p); }
-__device__ __forceinline__ void st2(u64* p, ulonglong2 v) { *reinterpret_cast<ulonglong2*>(p) = v; }
 __device__ __forceinline__ ulonglong2 ldg2(const u64* p) { return __ldg(reinterpret_cast<const ulonglong2*>(p)); }
 
 __device__ __forceinline__ u64 digit_of(const u32* __restrict__ limbs, u64 ndig, u64 n) {
