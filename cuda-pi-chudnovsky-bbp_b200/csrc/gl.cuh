@@ -267,19 +267,13 @@ __device__ __forceinline__ u64 gl_shl_160(u64 x, int t) {
     return gl_sub(((u64)(W2 + c) << 32) | l, (u64)W0 << 32);
 }
 
-// x * 2^s for x < 2^64 and a run-time, warp-uniform 0 <= s < 192: one copy
-// of the three word-offset folds behind uniform branches (t = 0 needs no
-// case of its own: the funnel shifts give W2 = 0 and the folds stay exact),
-// so a site costs a few hundred bytes of code instead of one specialised
-// body per shift amount.
-static __device__ __noinline__ u64 gl_shl_rt(u64 x, u32 s) {
 #if defined(__CUDA_ARCH__)
-    const bool neg = s >= 96;
-    if (neg) s -= 96;
-    const u32 t = s & 31, w = s >> 5;
+// x * 2^(32w + t) for a word offset w in {0, 1, 2} and 0 <= t < 32, the three
+// folds of the run-time shift (t = 0 needs no case of its own: the funnel
+// shifts give W2 = 0 and the folds stay exact).
+__device__ __forceinline__ u64 gl_shl_wt(u64 x, u32 w, u32 t) {
     const u32 x0 = (u32)x, x1 = (u32)(x >> 32);
     const u32 W0 = x0 << t, W1 = __funnelshift_l(x0, x1, t), W2 = __funnelshift_l(x1, 0u, t);
-    u64 r;
     if (w == 0) {
         const u64 L = ((u64)W1 << 32) | W0;
         u64 T;
@@ -288,19 +282,58 @@ static __device__ __noinline__ u64 gl_shl_rt(u64 x, u32 s) {
         asm("add.cc.u32 %0, %3, -1;\n\taddc.cc.u32 %1, %4, 0;\n\taddc.u32 %2, 0, 0;"
             : "=r"(e0), "=r"(e1), "=r"(c)
             : "r"((u32)T), "r"((u32)(T >> 32)));
-        r = ((T < L) | c) ? (((u64)e1 << 32) | e0) : T;
+        return ((T < L) | c) ? (((u64)e1 << 32) | e0) : T;
     } else if (w == 1) {
         u32 h, hc;
         asm("add.cc.u32 %0, %2, %3;\n\taddc.u32 %1, 0, 0;" : "=r"(h), "=r"(hc) : "r"(W0), "r"(W1));
-        r = gl_sub(((u64)h << 32) | (0u - hc), (u64)W1 + W2);
+        return gl_sub(((u64)h << 32) | (0u - hc), (u64)W1 + W2);
     } else {
         u32 l, c;
         asm("add.cc.u32 %0, %2, %3;\n\taddc.u32 %1, 0, 0;" : "=r"(l), "=r"(c) : "r"(W0), "r"(W1));
-        r = gl_sub((u64)W0 << 32, ((u64)(W2 + c) << 32) | l);
+        return gl_sub((u64)W0 << 32, ((u64)(W2 + c) << 32) | l);
     }
+}
+#endif
+
+// x * 2^s for x < 2^64 and a run-time, warp-uniform 0 <= s < 192: one copy
+// of the three word-offset folds behind uniform branches, so a site costs a
+// few hundred bytes of code instead of one specialised body per shift amount.
+static __device__ __noinline__ u64 gl_shl_rt(u64 x, u32 s) {
+#if defined(__CUDA_ARCH__)
+    const bool neg = s >= 96;
+    if (neg) s -= 96;
+    const u64 r = gl_shl_wt(x, s >> 5, s & 31);
     return neg ? gl_sub(0, r) : r;
 #else
     return gl_shl(x, (int)s);
+#endif
+}
+
+// The same shift of two values (one call, one decode of s): the paired
+// inverse tile tasks shift both columns' elements by the same amount.
+static __device__ __noinline__ ulonglong2 gl_shl_rt2(u64 x, u64 y, u32 s) {
+#if defined(__CUDA_ARCH__)
+    const bool neg = s >= 96;
+    if (neg) s -= 96;
+    const u32 w = s >> 5, t = s & 31;
+    u64 rx, ry;
+    if (w == 0) {
+        rx = gl_shl_wt(x, 0, t);
+        ry = gl_shl_wt(y, 0, t);
+    } else if (w == 1) {
+        rx = gl_shl_wt(x, 1, t);
+        ry = gl_shl_wt(y, 1, t);
+    } else {
+        rx = gl_shl_wt(x, 2, t);
+        ry = gl_shl_wt(y, 2, t);
+    }
+    if (neg) {
+        rx = gl_sub(0, rx);
+        ry = gl_sub(0, ry);
+    }
+    return make_ulonglong2(rx, ry);
+#else
+    return make_ulonglong2(gl_shl(x, (int)s), gl_shl(y, (int)s));
 #endif
 }
 

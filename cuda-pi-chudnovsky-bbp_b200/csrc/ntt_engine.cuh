@@ -285,6 +285,24 @@ __device__ __forceinline__ void level1_twiddle(u64* x, int u1) {
     }
 }
 
+// Both columns of a paired task: one run-time shift call per element pair.
+template <bool INV, bool RT>
+__device__ __forceinline__ void level1_twiddle2(u64* x, u64* y, int u1) {
+    if constexpr (RT) {
+        if (u1 == 0) return;
+#pragma unroll
+        for (int i = 1; i < 8; ++i) {
+            const u32 s = (u32)(3 * brev_c(i, 3)) * (u32)u1;  // < 192
+            const ulonglong2 r = gl_shl_rt2(x[i], y[i], INV ? 192u - s : s);
+            x[i] = r.x;
+            y[i] = r.y;
+        }
+    } else {
+        level1_twiddle<INV, RT>(x, u1);
+        level1_twiddle<INV, RT>(y, u1);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Radix-64 group on blocks of L = 2^LOGL rows: instance (col, blk, j) with
 // j in [0, L/64) owns rows blk*L + j + u*(L/64), u in [0, 64), u = u1 + 8*u2.
@@ -320,11 +338,9 @@ __device__ __forceinline__ void group64(u64* sm, const u64* __restrict__ dtw) {
                 if (!INV) {
                     dft_fwd<8, ZH>(x);
                     dft_fwd<8, ZH>(y);
-                    level1_twiddle<false, RT>(x, u1);
-                    level1_twiddle<false, RT>(y, u1);
+                    level1_twiddle2<false, RT>(x, y, u1);
                 } else {
-                    level1_twiddle<true, RT>(x, u1);
-                    level1_twiddle<true, RT>(y, u1);
+                    level1_twiddle2<true, RT>(x, y, u1);
                     dft_inv<8>(x);
                     dft_inv<8>(y);
                 }
