@@ -349,6 +349,43 @@ __device__ __forceinline__ void group64(u64* sm, const u64* __restrict__ dtw) {
             });
             return;
         }
+        if constexpr (RT && TL::LC >= 1) {
+            // run-time shifts: a thread's two tasks are instances inst and
+            // inst + NI/2 of the same u1, so one call shifts both (tiles of
+            // one column, the single-CTA products among them, keep single
+            // tasks: two live tasks there spill)
+            for_tasks<TASKS / 2, TL::T>([&](int p) {
+                const int u1 = p >> (LOGNI - 1);
+                const int inst = p & (NI / 2 - 1);
+                int col, blk, j;
+                TL::template decode<LOGJ>(inst, col, blk, j);
+                u64* ptr0 = sm + TL::saddr(blk * L + j + u1 * JW, col);
+                TL::template decode<LOGJ>(inst + NI / 2, col, blk, j);
+                u64* ptr1 = sm + TL::saddr(blk * L + j + u1 * JW, col);
+                constexpr int st = TL::template step<8 * JW>();
+                u64 x[8], y[8];
+#pragma unroll
+                for (int m = 0; m < (ZH ? 4 : 8); ++m) {
+                    x[m] = ptr0[m * st];
+                    y[m] = ptr1[m * st];
+                }
+                if (!INV) {
+                    dft_fwd<8, ZH>(x);
+                    dft_fwd<8, ZH>(y);
+                    level1_twiddle2<false, true>(x, y, u1);
+                } else {
+                    level1_twiddle2<true, true>(x, y, u1);
+                    dft_inv<8>(x);
+                    dft_inv<8>(y);
+                }
+#pragma unroll
+                for (int m = 0; m < 8; ++m) {
+                    ptr0[m * st] = x[m];
+                    ptr1[m * st] = y[m];
+                }
+            });
+            return;
+        }
         for_tasks<TASKS, TL::T>([&](int q) {
             const int u1 = q >> LOGNI;
             int col, blk, j;
