@@ -574,7 +574,17 @@ __device__ __forceinline__ void groups_inv(u64* sm, const u64* dtw) {
 // operand holding at most N/2 digits), so the first butterfly level of the
 // column DFT -- in the lead step, or in the first group when there is none --
 // has no additions and its zero half is not read.
-template <class TL, bool RT = (Steps<TL::LR>::G >= 2), bool ZH = false>
+// Level-1 twiddle form of a forward tile: run-time shifts where the tile has
+// two radix-64 groups, or one group and a lone radix-8 level in 2^9 rows of
+// two or more columns (two tasks per call: fwd_mid<9> 0.488 -> 0.469 ms at
+// 2^26 points); the eight specialised bodies elsewhere (2^8-row tiles
+// measured 4-6% slower with run-time shifts).
+template <class TL>
+constexpr bool fwd_rt() {
+    return Steps<TL::LR>::G >= 2 || (TL::LR == 9 && TL::LC >= 1);
+}
+
+template <class TL, bool RT = fwd_rt<TL>(), bool ZH = false>
 __device__ __forceinline__ void tile_fwd(u64* sm, const u64* dtw) {
     using S = Steps<TL::LR>;
     if constexpr (S::A > 0) {

@@ -203,7 +203,7 @@ k_fwd_first(const u32* __restrict__ limbs, u64 ndig, u64* __restrict__ out, int 
         if constexpr (TL::LC >= 1) load_digit_pairs<4>(sm, ColPair<TL>(logS), limbs, ndig);  // rows < R/2
         else load_digits<G::PER / 2>(sm, gp, limbs, ndig);  // rows row0 + k*DR < R/2
         __syncthreads();
-        tile_fwd<TL, (Steps<LOGR>::G >= 2), true>(sm, tw.dtw);
+        tile_fwd<TL, fwd_rt<TL>(), true>(sm, tw.dtw);
     } else {
         if constexpr (TL::LC >= 1) load_digit_pairs<8>(sm, ColPair<TL>(logS), limbs, ndig);
         else load_digits<G::PER>(sm, gp, limbs, ndig);
