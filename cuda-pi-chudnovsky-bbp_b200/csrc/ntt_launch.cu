@@ -50,10 +50,10 @@ constexpr DefaultPlan kDefaultPlans[DEFAULT_MAX_LOGN - DEFAULT_MIN_LOGN + 1] = {
     {2, 9, 12, 0, 13},   // 2^21
     {3, 6, 8, 8, 12},    // 2^22
     {2, 10, 13, 0, 13},  // 2^23
-    {3, 8, 8, 8, 12},    // 2^24
+    {3, 9, 9, 6, 12},    // 2^24
     {3, 9, 8, 8, 12},    // 2^25
     {3, 9, 9, 8, 12},    // 2^26
-    {3, 8, 8, 11, 12},   // 2^27
+    {3, 6, 9, 12, 12},   // 2^27
 };
 }  // namespace
 
