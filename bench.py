@@ -377,7 +377,7 @@ def run_ours(args) -> None:
                          "algorithmic_bytes_per_launch": dom_bytes, "avg_launch_ms": round(dom_ms, 4),
                          "peak_source": peak_src,
                          # what the ncu captures show holds the transform kernels
-                         "binding_unit": "integer ALU pipe, 77-84% of its peak in every transform kernel "
+                         "binding_unit": "integer ALU pipe, 79-83% of its peak in every transform kernel "
                                          "(ncu; profiles/kernels_2e23_instructions_traffic.md)",
                          "product": {"algorithmic_bytes": prod_bytes,
                                      "achieved_gbs": round(prod_bytes / (step_ms * 1e-3) / 1e9, 1),
