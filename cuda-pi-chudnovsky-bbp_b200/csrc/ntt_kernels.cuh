@@ -476,8 +476,8 @@ __global__ void __launch_bounds__(small_threads(LOGN), small_min_blocks(LOGN)) k
     }
     if (threadIdx.x == 0) s_top = 0;
     __syncthreads();
-    tile_fwd<TL>(smA, tw.dtw);
-    tile_fwd<TL>(smB, tw.dtw);
+    tile_fwd<TL, true>(smA, tw.dtw);
+    tile_fwd<TL, true>(smB, tw.dtw);
     for (int i = threadIdx.x; i < N; i += blockDim.x) {
         const int s = TL::saddr(i, 0);
         smB[s] = gl_mul(gl_mul(smB[s], smA[s]), ninv);
