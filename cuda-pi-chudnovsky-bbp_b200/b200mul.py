@@ -220,7 +220,7 @@ def selftest_wait_timeout(stream: int = 0) -> int:
 
 
 _sig("b2m_field_eval_host", ctypes.c_int, [ctypes.c_int, _u64p, _u64p, _u64p, ctypes.c_uint64])
-FIELD_OPS = {"add": 0, "sub": 1, "mul": 2, "shl": 3, "pow": 4, "inv": 5, "dft8": 6, "idft8": 7, "shl_rt": 8, "shl_160": 9}
+FIELD_OPS = {"add": 0, "sub": 1, "mul": 2, "shl": 3, "pow": 4, "inv": 5, "dft8": 6, "idft8": 7, "shl_rt": 8, "shl_160": 9, "shl_rt2": 10}
 
 
 def field_eval(op: str, a, b=None) -> np.ndarray:

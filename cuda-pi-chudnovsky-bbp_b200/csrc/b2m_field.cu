@@ -44,6 +44,13 @@ __global__ void k_field_eval(int op, const u64* __restrict__ a, const u64* __res
             case B2M_FIELD_INV: r = gl_inv(x); break;
             case B2M_FIELD_SHL_RT: r = gl_shl_rt(x, (u32)(y % 192)); break;
             case B2M_FIELD_SHL_160: r = gl_shl_160(x, (int)(y % 32)); break;
+            case B2M_FIELD_SHL_RT2: {
+                // elements 2k and 2k+1 shifted together by b[2k]
+                const u64 k0 = i & ~1ull;
+                const ulonglong2 q = gl_shl_rt2(a[k0], k0 + 1 < n ? a[k0 + 1] : 0, (u32)(b[k0] % 192));
+                r = (i & 1) ? q.y : q.x;
+                break;
+            }
             default: r = 0; break;
         }
         out[i] = r;
@@ -57,7 +64,7 @@ using namespace b2m;
 extern "C" b2m_status b2m_field_eval_host(int op, const uint64_t* a, const uint64_t* b, uint64_t* out, uint64_t n) {
     if (n == 0) return B2M_OK;
     const bool dft = op == B2M_FIELD_DFT8 || op == B2M_FIELD_IDFT8;
-    if (!a || !out || (!dft && !b) || op < 0 || op > B2M_FIELD_SHL_160 || (dft && (n % 8) != 0)) {
+    if (!a || !out || (!dft && !b) || op < 0 || op > B2M_FIELD_SHL_RT2 || (dft && (n % 8) != 0)) {
         set_error("b2m_field_eval_host: bad op, pointer or length");
         return B2M_ERR_INVALID_ARGUMENT;
     }

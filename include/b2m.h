@@ -152,7 +152,8 @@ typedef enum b2m_field_op {
     B2M_FIELD_DFT8 = 6,
     B2M_FIELD_IDFT8 = 7,
     B2M_FIELD_SHL_RT = 8,  /* a * 2^(b mod 192) by the run-time shift of the level-1 twiddles */
-    B2M_FIELD_SHL_160 = 9  /* a * 2^(160 + (b mod 32)): the carry's scale by N^-1 = 2^(192 - log2 N) */
+    B2M_FIELD_SHL_160 = 9, /* a * 2^(160 + (b mod 32)): the carry's scale by N^-1 = 2^(192 - log2 N) */
+    B2M_FIELD_SHL_RT2 = 10 /* a[2k], a[2k+1] * 2^(b[2k] mod 192) by the paired run-time shift */
 } b2m_field_op;
 b2m_status b2m_field_eval_host(int op, const uint64_t* a, const uint64_t* b, uint64_t* out, uint64_t n);
 

@@ -72,6 +72,24 @@ def test_every_shift_amount(b2m_gpu):
     assert ints(b2m_gpu.field_eval("shl_160", arr(xs), arr(ts))) == [(x << (160 + t)) % P for x, t in zip(xs, ts)]
 
 
+def test_paired_run_time_shift(b2m_gpu):
+    """The paired run-time shift of the inverse tile tasks: elements 2k and
+    2k+1 shifted together by b[2k], every amount 0..191, crossed edge values."""
+    rng = np.random.default_rng(193)
+    vals = EDGE + [int(v) % P for v in rng.integers(0, 2**63, 24, dtype=np.uint64)]
+    xs, ss = [], []
+    for i, x in enumerate(vals):
+        y = vals[(7 * i + 3) % len(vals)]
+        for s in range(192):
+            xs += [x, y]
+            ss += [s, 191 - s]  # the second amount is ignored: both take b[2k]
+    want = [(x << ss[i & ~1]) % P for i, x in enumerate(xs)]
+    assert ints(b2m_gpu.field_eval("shl_rt2", arr(xs), arr(ss))) == want
+    # odd length: the last element is shifted alone
+    got = ints(b2m_gpu.field_eval("shl_rt2", arr(xs[:5]), arr(ss[:5])))
+    assert got == want[:5]
+
+
 def test_random_pairs(b2m_gpu):
     rng = np.random.default_rng(100000)
     n = 100000
