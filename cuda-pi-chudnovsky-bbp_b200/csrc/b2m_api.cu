@@ -230,7 +230,7 @@ uint64_t b2m_workspace_bytes(uint64_t na, uint64_t nb) {
     Context* c = ctx();
     int logn = 0, three = 0;
     choose_length(2 * (na + nb), &logn, &three);
-    Plan p = c ? plan_for(c, logn) : make_plan(logn);
+    Plan p = c ? plan_for(c, logn, three) : make_plan(logn, three);
     p.three = three;
     return workspace_bytes_plan(p);
 }
@@ -279,7 +279,7 @@ b2m_status b2m_plan_describe(uint64_t na, uint64_t nb, b2m_plan_desc* d) {
     Context* c = ctx();
     int l = 0, three = 0;
     choose_length(2 * (na + nb), &l, &three);
-    Plan p = c ? plan_for(c, l) : make_plan(l);
+    Plan p = c ? plan_for(c, l, three) : make_plan(l, three);
     p.three = three;
     d->ntt_log2 = (uint32_t)l;
     d->three = (uint32_t)three;

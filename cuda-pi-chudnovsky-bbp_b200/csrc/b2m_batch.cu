@@ -222,8 +222,7 @@ b2m_status b2m_batch_create(const b2m_job* jobs, uint64_t njobs, uint32_t flags,
       for (size_t off = 0; off < it->second.size(); off += MAX_GRID_Y) {
         Bucket b;
         b.logn = lg;
-        b.plan = plan_for(c, b.logn);
-        b.plan.three = three;
+        b.plan = plan_for(c, b.logn, three);
         b.first = (unsigned)hj.size();
         b.njobs = (unsigned)std::min<size_t>(MAX_GRID_Y, it->second.size() - off);
         for (size_t k = off; k < off + b.njobs; ++k) {

@@ -575,9 +575,7 @@ static cudaError_t merge_level(Context* c, const LevelView& L, const uint64_t mx
     auto kind_plan = [&](int k) {
         int logn = 0, three = 0;
         choose_length(2 * cap[k], &logn, &three);
-        Plan p = plan_for(c, logn);
-        p.three = three;
-        return p;
+        return plan_for(c, logn, three);
     };
     // Pairs that share a forward spectrum: Q = QR*QL then X = QR*TL (QR), and
     // P = PL*PR then Y = PL*TR (PL). A shared pair runs both products under

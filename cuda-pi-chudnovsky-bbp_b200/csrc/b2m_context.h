@@ -50,10 +50,13 @@ struct Context {
     }
 };
 
-// The plan products of transform length 2^logn use: the tuned one if any.
-inline Plan plan_for(Context* c, int logn) {
+// The plan products of (sub-)transform length 2^logn use: the tuned one if
+// any, else the default (three: the radix-3 products' default).
+inline Plan plan_for(Context* c, int logn, int three = 0) {
     std::lock_guard<std::mutex> lk(c->tune_mu);
-    return c->has_tuned[logn] ? c->tuned[logn] : make_plan(logn);
+    Plan p = c->has_tuned[logn] ? c->tuned[logn] : make_plan(logn, three);
+    p.three = three;
+    return p;
 }
 // The plan of an na x nb product: 2^L points, or 3 * 2^(L-2) when that holds
 // the 2(na + nb) digits (choose_length), its sub-transform the tuned or
@@ -61,9 +64,7 @@ inline Plan plan_for(Context* c, int logn) {
 inline Plan product_plan(Context* c, uint64_t na, uint64_t nb) {
     int logn = 0, three = 0;
     choose_length(2 * (na + nb), &logn, &three);
-    Plan p = plan_for(c, logn);
-    p.three = three;
-    return p;
+    return plan_for(c, logn, three);
 }
 inline void set_tuned(Context* c, int logn, const Plan& p) {
     std::lock_guard<std::mutex> lk(c->tune_mu);

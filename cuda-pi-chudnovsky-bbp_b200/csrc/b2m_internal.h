@@ -51,7 +51,9 @@ constexpr int RADIX3_MIN_LOG = 14;
 // convolution output (2na + 2nb): three = 1 when 3 * 2^(L-2) >= digits.
 void choose_length(uint64_t digits, int* logn, int* three);
 
-Plan make_plan(int logn);
+// The default plan of a 2^logn-point transform, or (three) of the 2^logn-point
+// sub-transforms of a 3 * 2^logn-point product.
+Plan make_plan(int logn, int three = 0);
 Plan make_plan_custom(int logn, int r0, int tile);
 Plan make_plan_split(int logn, const int* r, int npass, int tile);
 std::vector<Plan> plan_candidates(int logn);

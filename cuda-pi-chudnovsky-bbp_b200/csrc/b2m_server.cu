@@ -246,8 +246,7 @@ static cudaError_t launch_dispatch(b2m_server* S, Slot& sl, std::vector<Req>& rv
         const uint64_t pts = rs[order[k0]]->pts;
         size_t k1 = k0;
         while (k1 < n && rs[order[k1]]->pts == pts && k1 - k0 < 65535) ++k1;
-        Plan p = plan_for(S->c, rs[order[k0]]->logn);
-        p.three = rs[order[k0]]->three;
+        Plan p = plan_for(S->c, rs[order[k0]]->logn, rs[order[k0]]->three);
         if ((e = twtable_ensure(S->c, p, s)) != cudaSuccess) return e;
         if ((e = launch_bucket(p, djobs + k0, (unsigned)(k1 - k0), S->c->tw, S->c->d_err, s)) != cudaSuccess) return e;
         // Residue check of the bucket's products, its grid sized to the
@@ -418,6 +417,10 @@ b2m_status b2m_server_start(const b2m_server_config* cfg, b2m_server** out) {
         const uint64_t pts = 1ull << logn;
         if (2 * 8 * pts > S->cfg.hbm_budget_bytes) break;
         if (twtable_ensure(c, plan_for(c, logn), S->release_stream) != cudaSuccess) break;
+        // the sub-transform plan of 3 * 2^logn points may differ
+        if (6 * 8 * pts <= S->cfg.hbm_budget_bytes &&
+            twtable_ensure(c, plan_for(c, logn, 1), S->release_stream) != cudaSuccess)
+            break;
     }
     // Each slot's arena starts at an equal share of half the budget (at most
     // 4 GiB), so that typical dispatches never grow it.

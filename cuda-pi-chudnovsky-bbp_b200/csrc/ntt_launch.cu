@@ -57,7 +57,31 @@ constexpr DefaultPlan kDefaultPlans[DEFAULT_MAX_LOGN - DEFAULT_MIN_LOGN + 1] = {
 };
 }  // namespace
 
-Plan make_plan(int logn) {
+// Sub-transform plans of 3 * 2^logn-point products where the autotuner's
+// fastest differs from the power-of-two default (measured on a B200 with
+// na = nb = 3 * 2^(logn-2) limbs): the radix-3 step already adds a pass, and
+// three shorter passes beat two long ones (2^23: [10, 13] 1.887 ms ->
+// [9, 6, 8] 1.770 ms; 2^21: [9, 12] 0.502 -> [9, 6, 6] 0.471 ms).
+struct Radix3Plan {
+    int logn, npass, r0, r1, r2;
+};
+constexpr Radix3Plan kRadix3Plans[] = {
+    {15, 2, 8, 7, 0}, {19, 2, 8, 11, 0}, {21, 3, 9, 6, 6}, {23, 3, 9, 6, 8},
+};
+
+Plan make_plan(int logn, int three) {
+    if (three) {
+        for (const Radix3Plan& d : kRadix3Plans)
+            if (d.logn == logn) {
+                const int r[3] = {d.r0, d.r1, d.r2};
+                Plan p = make_plan_split(logn, r, d.npass, 12);
+                p.three = 1;
+                return p;
+            }
+        Plan p = make_plan(logn, 0);
+        p.three = 1;
+        return p;
+    }
     if (logn <= SMALL_MAX_LOGN) return make_plan_split(logn, nullptr, 0, -1);
     if (logn >= DEFAULT_MIN_LOGN && logn <= DEFAULT_MAX_LOGN) {
         const DefaultPlan& d = kDefaultPlans[logn - DEFAULT_MIN_LOGN];
