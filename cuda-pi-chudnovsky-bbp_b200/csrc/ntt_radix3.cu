@@ -51,6 +51,21 @@ __global__ void __launch_bounds__(256) k_r3_fwd(const u32* __restrict__ limbs, u
         out = operand ? J.bufB : J.bufA;
     }
     const u64 m = 1ull << logm;
+    if (2 * ndig <= 3 * m) {
+        // The digits fill at most half of the 3m points (N >= 2(na + nb)
+        // digits for every product), so x2 = x[j + 2m] is zero: three outputs
+        // from x0 and x1 alone.
+        for (u64 j = (u64)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (u64)gridDim.x * blockDim.x) {
+            const u64 x0 = digit_of(limbs, ndig, j), x1 = digit_of(limbs, ndig, j + m);
+            u32 xm, x3;
+            w_exp(j, logm, &xm, &x3);
+            const u64 w1 = omega_pow(xm, x3, tw);
+            out[j] = gl_add(x0, x1);
+            out[m + j] = gl_mul(gl_add(x0, gl_shl(x1, 64)), w1);                  // (x0 + w x1) W^j
+            out[2 * m + j] = gl_mul(gl_add(x0, gl_shl(x1, 128)), gl_mul(w1, w1));  // (x0 + w^2 x1) W^2j
+        }
+        return;
+    }
     for (u64 j = (u64)blockIdx.x * blockDim.x + threadIdx.x; j < m; j += (u64)gridDim.x * blockDim.x) {
         const u64 x0 = digit_of(limbs, ndig, j), x1 = digit_of(limbs, ndig, j + m),
                   x2 = digit_of(limbs, ndig, j + 2 * m);
