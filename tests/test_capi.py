@@ -78,3 +78,18 @@ def test_empty_operand_is_empty_product_without_device():
     # reference: mul_ntt_cuda returns {} for an empty input (src/ntt_cuda.cu:181)
     a = np.ones(3, np.uint32)
     assert b200mul.mul_ntt_cuda(a, np.zeros(0, np.uint32)).size == 0
+
+
+def test_default_plans_without_device():
+    """Default plans (no context, no GPU): the measured power-of-two plan of
+    the 2^26-point headline, the radix-3 sub-transform plans where they
+    differ from it, and the power-of-two plan where no radix-3 entry exists."""
+    d = b200mul.plan_describe(1 << 24, 1 << 24)
+    assert (d["three"], d["ntt_log2"], d["logr"]) == (0, 26, [9, 9, 8])
+    d = b200mul.plan_describe(3 << 21, 3 << 21)  # 3 * 2^23 points
+    assert (d["three"], d["ntt_log2"], d["logr"], d["logc"]) == (1, 23, [9, 6, 8], [3, 6, 4])
+    d = b200mul.plan_describe(3 << 19, 3 << 19)  # 3 * 2^21 points
+    assert (d["three"], d["ntt_log2"], d["logr"]) == (1, 21, [9, 6, 6])
+    d3 = b200mul.plan_describe(3 << 20, 3 << 20)  # 3 * 2^22 points: no radix-3 entry
+    d2 = b200mul.plan_describe(1 << 20, 1 << 20)  # 2^22 points
+    assert d3["three"] == 1 and d3["ntt_log2"] == d2["ntt_log2"] == 22 and d3["logr"] == d2["logr"]
